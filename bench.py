@@ -1,0 +1,380 @@
+#!/usr/bin/env python
+"""Benchmark of the plain FP64 LU + solve (lu2's lumcolumn) on B200.
+
+Workload (default): one dense FP64 system, N = 65536, block width nb = 256,
+recursive panels down to 16 columns, partial pivoting; A and b from lu2's
+seeded drand48 stream (randomsetmat, seed 1), generated on the device.  A
+step is one factor + solve of that system.  The 34 GB matrix exceeds the
+126 MB L2, so no flush is needed between steps.
+
+value  : (2/3 N^3 + 2 N^2) / t, device-resident inputs, CUDA events, max over
+         ranks; every step restores A from a pristine device copy (inside the
+         timed region) and runs factor + back substitution.
+e2e    : the same through the reference-facing C entry point lumcolumn() on
+         pinned host buffers: host->device copy of A|b, factor, solve,
+         device->host copy of the factors and x, all inside the timed region.
+roofline: the trailing-update DGEMM (the dominant kernel), its algorithmic
+         FLOPs over its CUDA-event time, against the FP64 DGEMM peak measured
+         with cuBLAS (torch.matmul float64, 8192^3) in the same run.
+cpu_baseline: the reference compiled from its own sources (oracle/_ref:
+         lu2.c/lu2tlib.c/lu2lib.c + OpenBLAS), lumcolumn at N = 8192, all host
+         cores.
+
+--impl reference times that same reference CPU build on a bounded sample
+(N = 8192) of the workload, on rank 0 only.
+Multi-GPU (--gpus N under torchrun): independent replicas, one system per GPU
+(LU has no natural sharding at this scope), weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "LU GFLOP/s at N=65536: FP64 vs BF16-LU+IR to FP64 residual; batched solves/s"
+UNIT = "GFLOP/s"
+REF_SAMPLE_N = 8192
+
+
+def lu_flops(n: int) -> float:
+    """Factor + solve FLOPs as the metric defines them: 2/3 N^3 + 2 N^2."""
+    return 2.0 / 3.0 * n**3 + 2.0 * n**2
+
+
+def trailing_flops(n: int, nb: int, nrhs: int = 1) -> float:
+    """Algorithmic FLOPs of the top-level trailing updates C -= L21 U12."""
+    f = 0.0
+    for i in range(0, n, nb):
+        w = min(nb, n - i)
+        m_rows = n - i - w
+        n_cols = n + nrhs - i - w
+        f += 2.0 * m_rows * n_cols * w
+    return f
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            p = [s.strip() for s in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                rows.append((float(p[1]), float(p[2]), float(p[3]), p[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        load = [r for r in rows if r[2] > 250.0] or rows
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in load for i, v in enumerate(r[3]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in load), "sm_max_mhz": max(r[1] for r in rows),
+                "power_w_median": statistics.median(r[2] for r in load), "samples": len(load),
+                "reasons": reasons}
+
+
+def cpu_reference_gflops(n: int, nb: int, runs: int) -> dict:
+    """The reference's own lumcolumn on the host cores (oracle/_ref), or the
+    oracle restatement if the reference was not compiled."""
+    cores = os.cpu_count() or 1
+    from oracle.oracle import OracleLib, RefLib
+
+    if RefLib.available("shipped"):
+        ref = RefLib("shipped")
+        ref.set_threads(cores, 1)
+        ts = []
+        for _ in range(runs):
+            _, t = ref.lumcolumn(n, nb, 1)
+            ts.append(t)
+        t = statistics.median(ts)
+        return {"value": lu_flops(n) / t / 1e9, "unit": UNIT, "cores": cores, "kind": "reference",
+                "sample": "lu2 lumcolumn (lu2.c:1122) compiled from the reference sources + OpenBLAS 0.3.15, "
+                          "N=%d nb=%d seed 1, %d OpenBLAS threads, median of %d" % (n, nb, cores, runs),
+                "seconds": ts}
+    orc = OracleLib()
+    n2 = 2048
+    a = orc.randomsetmat(n2, 1)
+    t0 = time.perf_counter()
+    orc.lumcolumn(a, n2, 64)
+    t = time.perf_counter() - t0
+    return {"value": lu_flops(n2) / t / 1e9, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": "oracle restatement N=%d nb=64" % n2}
+
+
+def fp64_peak(device) -> float:
+    """cuBLAS DGEMM 8192^3 (torch.matmul float64), best of 5, TFLOP/s."""
+    import torch
+
+    n = 8192
+    a = torch.rand((n, n), dtype=torch.float64, device=device)
+    b = torch.rand((n, n), dtype=torch.float64, device=device)
+    c = a @ b
+    best = 1e9
+    for _ in range(5):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b, out=c)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    del a, b, c
+    torch.cuda.empty_cache()
+    return 2.0 * n**3 / best / 1e12
+
+
+def read_profile_traffic():
+    """Per-launch DRAM traffic of the trailing-update kernel, from the committed
+    ncu summary (scaled to one full-size launch there), or None."""
+    p = os.path.join(ROOT, "profiles", "dgemm_update_fp64.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("traffic_bytes_per_launch_full_size:"):
+            try:
+                return float(line.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
+def run_reference(args, rank: int) -> None:
+    if rank != 0:
+        return
+    from oracle.oracle import RefLib
+
+    cores = os.cpu_count() or 1
+    n, nb = REF_SAMPLE_N, args.nb
+    if not RefLib.available("shipped"):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (the compiled reference) not present"}))
+        return
+    ref = RefLib("shipped")
+    ref.set_threads(cores, 1)
+    for _ in range(args.warmup):
+        ref.lumcolumn(n, nb, 1)
+    ts = []
+    for _ in range(args.steps):
+        _, t = ref.lumcolumn(n, nb, 1)
+        ts.append(t)
+    tot = sum(ts)
+    value = args.steps * lu_flops(n) / tot / 1e9
+    sample = ("lu2 lumcolumn compiled from the reference sources (lu2.c, lu2tlib.c, lu2lib.c) + OpenBLAS 0.3.15, "
+              "N=%d nb=%d seed 1 per step (bounded sample of the N=%d workload), %d threads" % (n, nb, args.n, cores))
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": "plain FP64 LU+solve (reference CPU lu2), N=%d sample of N=%d, nb=%d" %
+                                  (n, args.n, nb), "n": n, "nb": nb, "seed": 1},
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=65536)
+    ap.add_argument("--nb", type=int, default=256)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return 0
+
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
+
+    import numpy as np
+
+    import lu2_b200 as L
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v: float) -> float:
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    n, nb = args.n, args.nb
+    ctx = L.Context(local)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    ld = L.device_ld(n)
+    pristine = torch.empty((n, ld), dtype=torch.float64, device=dev)
+    A = torch.empty_like(pristine)
+    ctx.generate(pristine, n, ld, 1)
+    lib = L.load()
+    launches0 = lib.lu2gpu_kernel_launches()
+
+    def step():
+        A.copy_(pristine)
+        info = ctx.lusolve(A, n, ld, nb, 1, L.PIVOT_PARTIAL)
+        if info != 0:
+            raise RuntimeError("zero pivot at column %d" % (info - 1))
+
+    log("warmup x%d (n=%d nb=%d)" % (args.warmup, n, nb))
+    for _ in range(args.warmup):
+        step()
+    clocks = Clocks(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    launches0 = lib.lu2gpu_kernel_launches()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    launches = lib.lu2gpu_kernel_launches() - launches0
+    clk = clocks.stop()
+    barrier()
+    t = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    value = world * args.steps * lu_flops(n) / t / 1e9
+    log("timed: %.3f s for %d steps -> %.1f GFLOP/s" % (t, args.steps, value))
+
+    # accuracy of the last step: HPL scaled residual on the device (float64)
+    x = A[:, n].clone()
+    A0 = pristine[:, :n]
+    b0 = pristine[:, n]
+    r = (A0 @ x - b0).abs().max().item()
+    hplres = r / (2.0**-53 * (A0.abs().sum(1).max().item() * x.abs().max().item() + b0.abs().max().item()) * n)
+    del x
+
+    # instrumented step: per-phase CUDA-event timers (not part of the timed region)
+    ctx.set_timing(True)
+    step()
+    torch.cuda.synchronize()
+    timers = ctx.timers()
+    ctx.set_timing(False)
+    gemm_ms, gemm_launches = timers["DGEMMrest"]
+    gemm_flops = trailing_flops(n, nb)
+    achieved = gemm_flops / (gemm_ms / 1e3) / 1e12
+    peak = fp64_peak(dev)
+    roofline = {"bound": "tensor", "kernel": "dgemm_tn_kernel (trailing update C -= L21 U12)",
+                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "peak_source": "FP64 DGEMM measured in this run: cuBLAS via torch.matmul float64 8192^3, best of 5",
+                "traffic": read_profile_traffic(), "launches_per_step": gemm_launches,
+                "avg_launch_ms": gemm_ms / max(gemm_launches, 1),
+                "flops_per_step": gemm_flops}
+    phases = {k: {"ms": v[0], "launches": v[1]} for k, v in timers.items()}
+
+    # end to end through the reference-facing C entry point on pinned host memory
+    e2e = None
+    if not args.no_e2e:
+        del A
+        torch.cuda.empty_cache()
+        host = torch.empty((n, n + 16), dtype=torch.float64, pin_memory=True)
+        bvec = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        pv = np.zeros(nb, dtype=np.int32)
+        assert ld == n + 16, "device and host row strides differ"
+        lib.lu2gpu_set_stream(lib.lu2gpu_default_context(), stream.cuda_stream)
+        hn, bn = host.numpy(), bvec.numpy()
+        ts = []
+        for it in range(1 + args.e2e_steps):
+            host.copy_(pristine, non_blocking=False)  # untimed restore of the input
+            torch.cuda.synchronize()
+            barrier()
+            f0 = torch.cuda.Event(enable_timing=True)
+            f1 = torch.cuda.Event(enable_timing=True)
+            f0.record(stream)
+            rc = L.lumcolumn(hn, bn, nb, pv, L.PIVOT_PARTIAL)
+            f1.record(stream)
+            torch.cuda.synchronize()
+            if rc != 0:
+                raise RuntimeError("lumcolumn status %d" % rc)
+            if it > 0:
+                ts.append(f0.elapsed_time(f1) / 1e3)
+        te = max_over_ranks(sum(ts))
+        e2e = {"value": world * len(ts) * lu_flops(n) / te / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": n * (n + 1) * 8, "d2h_bytes_per_step": n * (n + 1) * 8 + n * 8 + nb * 4,
+               "steps": len(ts), "api": "lumcolumn() C entry point, pinned host buffers"}
+        lib.lu2gpu_release()
+        del host, bvec
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_reference_gflops(REF_SAMPLE_N, nb, 2)
+
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+               "config": {"workload": "plain FP64 LU+solve (lumcolumn), N=%d, nb=%d, panels split to 16, "
+                                      "partial pivoting, drand48 seed 1" % (n, nb),
+                          "n": n, "nb": nb, "leaf": 16, "pivoting": "partial", "seed": 1,
+                          "parallelism": "replicas" if world > 1 else "single",
+                          "l2": "inputs (%.1f GB) larger than L2, no flush" % (n * ld * 8 / 1e9)},
+               "gpu_launches": int(launches), "hpl_residual": hplres, "clocks": clk, "roofline": roofline,
+               "phases_ms": phases, "e2e": e2e, "cpu_baseline": cpu}
+        print(json.dumps(out))
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

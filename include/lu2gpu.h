@@ -1,0 +1,185 @@
+/*
+ * lu2gpu.h -- C ABI of liblu2gpu.so, the B200 (sm_100a) implementation of
+ * telmin/lu2's single-node blocked recursive LU with partial pivoting and its
+ * solve.
+ *
+ * Two groups of entry points:
+ *
+ *  1. lu2's own signatures, drop-in replacements for the functions a caller of
+ *     lu2 links against (paths within telmin/lu2).  All pointers are HOST
+ *     pointers, as in the reference; the library stages them through the GPU.
+ *     C99 VLA parameters of the reference (double a[n][n+16]) are ABI-identical
+ *     to the plain pointers declared here.
+ *
+ *  2. a handle-based API on DEVICE pointers (the performance path: the matrix
+ *     stays resident in HBM), returning int status codes.
+ *
+ * Status codes (group 2, and lu2gpu_lumcolumn): 0 ok; > 0 the factorization
+ * met an exact zero pivot at column (status - 1) and completed without
+ * scaling that column (LAPACK getrf's info convention); < 0 an error below.
+ * lu2gpu_last_error() describes the last failure of the calling thread.
+ *
+ * The reference's own entry points return void.  On failure they print the
+ * error and end the process (the reference's MP_error convention,
+ * lu2_mp_nompi.c:55-58) unless lu2gpu_set_abort_on_error(0) was called;
+ * gdr_dgemm_ instead reports through *doneflag = 0 (gdrdgemm.c:113-116).
+ * There is no CPU fallback.
+ *
+ * Storage (same as lu2, lu2.c:28): row-major, leading dimension in doubles,
+ * right-hand sides as augmented columns n..n+nrhs-1 that ride through every
+ * swap and update (lu2.c:1138).  Factors: unit upper U' (pivot rows scaled by
+ * 1/pivot, diagonal keeps the pivot) and L' below; earlier panels' L columns
+ * are not swapped by later panels (lu2.c:543-553).  The full pivot sequence is
+ * kept (0-based LAPACK ipiv order: row c was exchanged with row ipiv[c]).
+ */
+#ifndef LU2GPU_H
+#define LU2GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LU2GPU_OK 0
+#define LU2GPU_ERR_ARG (-1)
+#define LU2GPU_ERR_CUDA (-2)
+#define LU2GPU_ERR_NOMEM (-3)
+#define LU2GPU_ERR_TIMEOUT (-4) /* a bounded device wait gave up */
+#define LU2GPU_ERR_NODEV (-5)
+
+/* pivot search */
+#define LU2GPU_PIVOT_REF 0     /* bug-compatible with lu2tlib.c:1052 (see below) */
+#define LU2GPU_PIVOT_PARTIAL 1 /* true partial pivoting (default) */
+
+/* CBLAS enum values (CBLAS_ORDER / CBLAS_TRANSPOSE) accepted by gdrblas_dgemm */
+#define LU2GPU_CBLAS_ROWMAJOR 101
+#define LU2GPU_CBLAS_COLMAJOR 102
+#define LU2GPU_CBLAS_NOTRANS 111
+#define LU2GPU_CBLAS_TRANS 112
+
+/* ======================================================================
+ * 1. Reference signatures (host pointers)
+ * ====================================================================== */
+
+/* lu2.c:1122-1144.  In-place LU of a[n][n+16] (row-major, b in column n) with
+ * block size m (a multiple of 16), then backward substitution: x -> b[n].
+ * a receives the factors (y in column n); pv[0..m) the last panel's pivot
+ * rows, as the reference leaves them.  awork and recursive are accepted and
+ * unused.  Pivot mode: LU2GPU_PIVOT_PARTIAL unless lu2gpu_set_pivot_mode()
+ * or the environment variable LU2GPU_PIVOT=ref selects the reference's. */
+void lumcolumn(int n, double *a, double *b, int m, double *awork, int *pv, int recursive);
+
+/* lu2lib.h:9-19, lu2lib.c:2079-2136: row-major C = alpha*A*B + beta*C. */
+void mydgemm(int m, int n, int k, double alpha, double *a, int na, double *b, int nb, double beta, double *c,
+             int nc);
+
+/* lu2lib.h:2-7, lu2lib.c:1984-2077: C -= A*B, A (m x kk, stride n1),
+ * B (kk x n, stride n2), C (m x n, stride n3), row-major. */
+void matmul_for_small_nk(int n1, double *a, int n2, double *b, int n3, double *c, int m, int kk, int n);
+
+/* lu2lib.c:2138-2168: initialise the offload device and run its self-test.
+ * The GPU has no nb >= 2048 restriction; caller buffers are not touched. */
+void reset_gdr(int m, double *a, int nb, double *awork, int n);
+
+/* lu2lib.h:21-23: select the GPU (board id = CUDA device ordinal). */
+void gdrsetboardid(int boardid);
+/* lu2lib.c:2170-2178 board controls; accepted, no effect on a GPU. */
+void gdrsetnboards(int nboards);
+void gdrsetforceswapab(void);
+void gdrresetforceswapab(void);
+void gdrsetskipsendjmat(void);
+void gdrresetskipsendjmat(void);
+void set_matmul_msg_level(int level);
+void gdrdgemm_set_stress_factor(int x);
+
+/* The GRAPE-DR board library's symbols as gdrdgemm.c calls them
+ * (gdrdgemm.c:55-56, 105-110, 171, 185-186; no header in the reference).
+ * gdr_dgemm_: Fortran-style column-major C = alpha*op(A)*op(B) + beta*C,
+ * *nota / *notb = 1 for no transpose, *doneflag = 1 on success, 0 on failure. */
+void gdr_dgemm_(int *nota, int *notb, int *m, int *n, int *k, double *alpha, double *beta, int *lda, int *ldb,
+                int *ldc, const double *a, const double *b, double *c, int *doneflag);
+void gdr_init(void);
+void gdr_free(void);
+void gdrdgemm_set_procname(int procid);
+
+/* gdrdgemm.h:15-37: CBLAS-style DGEMM (order/trans take the CBLAS enum values). */
+void gdrblas_dgemm(int order, int transa, int transb, int M, int N, int K, double alpha, const double *A, int lda,
+                   const double *B, int ldb, double beta, double *C, int ldc);
+
+/* gdrdgemm.h:39-49: row-major C = alpha*A*B + beta*C. */
+void mygdrdgemm(int m, int n, int k, double alpha, double *a, int na, double *b, int nb, double beta, double *c,
+                int nc);
+
+/* gdrdgemm.h:11-13, gdrdgemm.c:17-58: identity x B == B self-test on three
+ * 2048x2048 host buffers, bounded to three attempts. */
+void gdr_check_and_restart(double *a, double *b, double *c);
+
+/* ======================================================================
+ * 2. Device-resident API
+ * ====================================================================== */
+
+typedef struct lu2gpu_ctx lu2gpu_ctx;
+
+/* One context per device; holds its stream, workspaces and pivot arrays. */
+int lu2gpu_create(lu2gpu_ctx **ctx, int device);
+int lu2gpu_destroy(lu2gpu_ctx *ctx);
+/* Run on the caller's CUDA stream (a cudaStream_t) instead of the context's own. */
+int lu2gpu_set_stream(lu2gpu_ctx *ctx, void *stream);
+
+/* Factor the n x (n+nrhs) augmented row-major device matrix a (leading
+ * dimension lda, even; a 16-byte aligned) in place with block size nb (a
+ * multiple of 16): recursive panels down to 16 columns, lu2's storage.  The
+ * right-hand-side columns come out forward-transformed (y).  ipiv (device,
+ * n ints, may be NULL) receives the pivot sequence.  Synchronous. */
+int lu2gpu_factor(lu2gpu_ctx *ctx, int n, int nrhs, double *a, long lda, int nb, int pivot_mode, int *ipiv);
+
+/* x = U'^{-1} y with the unit upper factor of a (lu2.c:110-116); y is the
+ * n x nrhs device block x (row stride ldx), overwritten by x. */
+int lu2gpu_backsolve(lu2gpu_ctx *ctx, int n, int nrhs, const double *a, long lda, double *x, long ldx);
+
+/* lumcolumn on device memory: factor, then solve; x overwrites columns n..n+nrhs-1. */
+int lu2gpu_lusolve(lu2gpu_ctx *ctx, int n, int nrhs, double *a, long lda, int nb, int pivot_mode, int *ipiv);
+
+/* randomsetmat (lu2.c:70-85) on the device, bit-identical to glibc
+ * srand48(seed)/drand48(): row i is n draws then b_i, each drand48()-0.5;
+ * further right-hand sides continue the stream after the matrix.
+ * kind 0: as lu2; kind 1: then a_ii = sum_j |a_ij| over the row (diagonally
+ * dominant).  nrhs >= 1. */
+int lu2gpu_generate(lu2gpu_ctx *ctx, int n, int nrhs, long seed, int kind, double *a, long lda);
+
+/* Row-major device DGEMM, C = alpha*A*B + beta*C (mydgemm's contract). */
+int lu2gpu_dgemm_dev(lu2gpu_ctx *ctx, int m, int n, int k, double alpha, const double *a, long lda, const double *b,
+                     long ldb, double beta, double *c, long ldc);
+
+/* Copy the context's last pivot sequence (n ints) to host memory. */
+int lu2gpu_copy_pivots(lu2gpu_ctx *ctx, int *ipiv_host, int n);
+
+/* lumcolumn with an explicit pivot mode and a status code instead of exit. */
+int lu2gpu_lumcolumn(int n, double *a, double *b, int m, int *pv, int pivot_mode);
+
+/* The context behind the reference-signature entry points (device set by
+ * gdrsetboardid, default 0); lu2gpu_release() frees it. */
+lu2gpu_ctx *lu2gpu_default_context(void);
+int lu2gpu_release(void);
+
+/* Pivot mode of lumcolumn (returns the previous mode). */
+int lu2gpu_set_pivot_mode(int mode);
+/* 1 (default): the reference's void entry points exit(-1) on failure; 0: they
+ * return after printing.  Returns the previous setting. */
+int lu2gpu_set_abort_on_error(int on);
+const char *lu2gpu_last_error(void);
+
+/* Per-phase CUDA-event timers (the GPU counterpart of lu2's timerlib):
+ * 0 "col dec t" panel, 1 "swaprows", 2 "solve tri", 3 "DGEMMrest" trailing
+ * update, 4 "backward_sub".  get_timers fills ms[] and counts[] (launches)
+ * for up to nmax phases, returns the number of phases. */
+int lu2gpu_set_timing(lu2gpu_ctx *ctx, int enable);
+int lu2gpu_get_timers(lu2gpu_ctx *ctx, double *ms, long *counts, int nmax, int reset);
+const char *lu2gpu_timer_name(int phase);
+
+/* Number of CUDA kernels this library has launched in the process so far. */
+long lu2gpu_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LU2GPU_H */

@@ -1,0 +1,123 @@
+// lu2gpu_internal.cuh -- shared declarations of the sm_100a LU library.
+//
+// Storage convention (same as lu2, lu2.c:28 and lu2.c:1122-1144): the matrix
+// is row-major, `ld` doubles per row, with the right-hand sides riding along
+// as the augmented columns n..n+nrhs-1.  Pivot rows are scaled by 1/pivot in
+// every column except the diagonal (unit upper U, lu2.c:551-552,
+// lu2tlib.c:1057-1059); L columns of earlier panels are not swapped by later
+// panels (lu2.c:543-553).  The full pivot sequence ipiv[0..n) (0-based, LAPACK
+// order) and dinv[c] = 1/pivot are kept on the device.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace lu2gpu {
+
+// device status words (int[4]) written by kernels
+//   [0] first zero pivot: column + 1 (atomicMin; INFO_NONE when none)
+//   [1] error bits below
+//   [2] where the first error happened (kernel id)
+enum : int {
+    ERR_BARRIER_TIMEOUT = 1,
+    ERR_MBAR_TIMEOUT = 2,
+    ERR_BAD_ARG = 4,
+};
+constexpr int INFO_NONE = 0x7f7f7f7f;  // memset byte 0x7f
+constexpr unsigned long long WAIT_LIMIT_NS = 2000000000ull;  // every device wait gives up after 2 s
+
+constexpr int PIVOT_REF = 0;       // lu2 as shipped: 2nd column of each 2-column leaf pivots on the 1st
+constexpr int PIVOT_PARTIAL = 1;   // partial pivoting
+constexpr int PIVOT_REF_FIRST = 2; // lu2tlib.c column_decomposition called directly on a wider slab:
+                                   // every column searches the slab's first column
+
+__device__ __forceinline__ unsigned long long globaltimer_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void record_error(int *status, int bit, int where)
+{
+    if (atomicOr(&status[1], bit) == 0) atomicExch(&status[2], where);
+}
+
+// (value, row) ordering for the pivot search: larger |a| wins, ties go to the
+// lower row index (cblas_idamax semantics, lu2tlib.c:47).
+__device__ __forceinline__ bool argmax_better(double v1, int i1, double v2, int i2)
+{
+    return v1 > v2 || (v1 == v2 && i1 < i2);
+}
+
+__device__ __forceinline__ void warp_argmax(double &v, int &i)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        double ov = __shfl_xor_sync(0xffffffffu, v, o);
+        int oi = __shfl_xor_sync(0xffffffffu, i, o);
+        if (argmax_better(ov, oi, v, i)) {
+            v = ov;
+            i = oi;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host-side launchers (all asynchronous on `st`)
+
+// process-wide count of this library's kernel launches (lu2gpu_kernel_launches)
+void count_launch(long k = 1);
+
+struct LeafBuffers {
+    double *xrow;   // [2][maxG][16]
+    double *xval;   // [2][maxG]
+    int *xidx;      // [2][maxG]
+    double *rowc;   // [2][16]
+    unsigned *bar;  // grid barrier counter
+};
+
+// Factor the leaf panel: rows c0..n-1, columns c0..c0+w-1 (w <= 16) of the
+// view `a` whose element (0,0) is global (goff, goff).  ipiv/dinv are indexed
+// by view column; ipiv receives global row numbers (view row + goff).
+cudaError_t launch_leaf(double *a, long ld, int n, int c0, int w, int mode, int goff, int *ipiv, double *dinv,
+                        const LeafBuffers &buf, int *status, int max_ctas, cudaStream_t st);
+int leaf_max_ctas(int device);
+
+// Apply the pivots k0..k1-1 (row k <-> row ipiv[k], in order) to columns
+// cs..ce-1 and, when `scale`, multiply row k by dinv[k] after its swap.
+// ipiv holds global rows; the view's row is ipiv[k] - goff.
+cudaError_t launch_laswp_scale(double *a, long ld, int k0, int k1, const int *ipiv, int goff, const double *dinv,
+                               int cs, int ce, bool scale, cudaStream_t st);
+
+// In place X := T^{-1} X for the unit lower triangle T = strict lower part of
+// a[r0..r0+K)[r0..r0+K) and X = a[r0..r0+K)[cs..ce); also writes
+// bt[(j-cs)*K + l] = X[l][j] (the transposed block row for the update GEMM).
+cudaError_t launch_trsm_unit_lower(double *a, long ld, int r0, int K, int cs, int ce, double *bt, cudaStream_t st);
+
+// C[m][n] -= sum_k A[m][k] * Bt[n][k], the trailing update.  A is the
+// row-major matrix starting at (a_row0, a_col0) of `a` (stride ld, rows < a_rows
+// exist); Bt is (N x K) row-major with stride K.  K % 16 == 0.
+cudaError_t launch_dgemm_update(const double *a, long ld, int a_rows, int a_row0, int a_col0, const double *bt,
+                                double *c, long ldc, int M, int N, int K, int *status, cudaStream_t st);
+
+// General C = alpha * X * Y^T + beta * C (row-major C, M x N), X (M x K) and Y
+// (N x K) both K-contiguous with strides ldx, ldy (device pointers).
+cudaError_t launch_dgemm_general(const double *x, long ldx, const double *y, long ldy, double *c, long ldc, int M,
+                                 int N, int K, double alpha, double beta, int *status, cudaStream_t st);
+
+// out[j][i] = in[i][j] for an (rows x cols) block; strides in doubles.
+cudaError_t launch_transpose(const double *in, long ldi, double *out, long ldo, int rows, int cols, cudaStream_t st);
+
+// x = U'^{-1} y for the unit upper triangle of a[0..n)[0..n) (lu2's backward_sub,
+// lu2.c:110-116); y (n x nrhs, row stride ldx) is overwritten by x.  For lu2's
+// own layout x = a + n, ldx = ld.
+cudaError_t launch_backsolve(const double *a, long ld, int n, int nrhs, double *x, long ldx, cudaStream_t st);
+
+// lu2's matrix generator (randomsetmat, lu2.c:70-85) on the device, bit-identical to
+// glibc drand48: row i holds draws i*(n+1) .. i*(n+1)+n (b_i last); extra
+// right-hand sides continue the stream.  kind 1 then sets a_ii = sum_j |a_ij|.
+cudaError_t launch_generate(double *a, long ld, int n, int nrhs, long seed, int kind, cudaStream_t st);
+
+}  // namespace lu2gpu

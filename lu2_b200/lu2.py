@@ -1,0 +1,182 @@
+"""Host-side mirror of lu2's interface over liblu2gpu.so.
+
+Names follow the reference (telmin/lu2): ``lumcolumn`` (lu2.c:1122),
+``mydgemm`` (lu2lib.c:2079), ``gdr_dgemm_`` / ``gdrblas_dgemm`` /
+``mygdrdgemm`` (gdrdgemm.c), ``randomsetmat`` (lu2.c:70).  Host arrays are
+numpy; device arrays are anything with a ``data_ptr()`` (torch CUDA tensors)
+or raw integer addresses.
+
+Every call goes through the C ABI; there is no CPU path.  Failures raise
+``Lu2GpuError`` carrying ``lu2gpu_last_error()``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+
+PIVOT_REF = 0
+PIVOT_PARTIAL = 1
+CBLAS_ROWMAJOR, CBLAS_COLMAJOR, CBLAS_NOTRANS, CBLAS_TRANS = 101, 102, 111, 112
+TIMER_NAMES = ["col dec t", "swaprows", "solve tri", "DGEMMrest", "backward_sub"]
+
+
+class Lu2GpuError(RuntimeError):
+    def __init__(self, where: str, rc: int):
+        super().__init__("%s failed (status %d): %s" % (where, rc, _lib.last_error()))
+        self.rc = rc
+
+
+class SingularMatrix(Lu2GpuError):
+    """The factorization met an exact zero pivot (status = column + 1)."""
+
+
+def _check(where: str, rc: int) -> int:
+    if rc < 0:
+        raise Lu2GpuError(where, rc)
+    return rc
+
+
+def _ptr(x) -> int:
+    if x is None:
+        return 0
+    if isinstance(x, int):
+        return x
+    if isinstance(x, np.ndarray):
+        return x.ctypes.data
+    return int(x.data_ptr())
+
+
+def lib():
+    return _lib.load()
+
+
+def rdim(n: int) -> int:
+    """Row stride of lu2's augmented matrix (RDIM, lu2.c:28)."""
+    return n + 16
+
+
+# ---------------------------------------------------------------------------
+# reference entry points on host arrays
+
+
+def lumcolumn(a: np.ndarray, b: np.ndarray, nb: int, pv: np.ndarray | None = None,
+              pivot_mode: int = PIVOT_PARTIAL) -> int:
+    """lu2.c:1122-1144 on host memory: ``a`` is (n, n+16) row-major float64 with
+    b in column n; on return ``b`` holds x, ``a`` the factors.  Returns 0 or the
+    zero-pivot status (column + 1)."""
+    n = a.shape[0]
+    if a.dtype != np.float64 or not a.flags.c_contiguous or a.shape[1] != rdim(n):
+        raise ValueError("a must be a C-contiguous float64 (n, n+16) array")
+    if b.dtype != np.float64 or b.shape[0] < n or not b.flags.c_contiguous:
+        raise ValueError("b must be a contiguous float64 vector of length n")
+    if pv is None:
+        pv = np.zeros(nb, dtype=np.int32)
+    rc = lib().lu2gpu_lumcolumn(n, _ptr(a), _ptr(b), nb, _ptr(pv), pivot_mode)
+    return _check("lumcolumn", rc)
+
+
+def mydgemm(m, n, k, alpha, a, na, b, nb, beta, c, nc) -> None:
+    """Row-major C = alpha*A*B + beta*C on host arrays (lu2lib.c:2079)."""
+    lib().mydgemm(m, n, k, alpha, _ptr(a), na, _ptr(b), nb, beta, _ptr(c), nc)
+    err = _lib.last_error()
+    if err and "mydgemm" in err:
+        raise Lu2GpuError("mydgemm", -2)
+
+
+def gdr_dgemm_(nota, notb, m, n, k, alpha, beta, lda, ldb, ldc, a, b, c) -> int:
+    """The board library's Fortran-style column-major DGEMM; returns doneflag."""
+    I = C.c_int
+    D = C.c_double
+    done = I(0)
+    lib().gdr_dgemm_(C.byref(I(nota)), C.byref(I(notb)), C.byref(I(m)), C.byref(I(n)), C.byref(I(k)),
+                     C.byref(D(alpha)), C.byref(D(beta)), C.byref(I(lda)), C.byref(I(ldb)), C.byref(I(ldc)),
+                     _ptr(a), _ptr(b), _ptr(c), C.byref(done))
+    return done.value
+
+
+def gdrblas_dgemm(order, transa, transb, M, N, K, alpha, A, lda, B, ldb, beta, Cm, ldc) -> None:
+    lib().gdrblas_dgemm(order, transa, transb, M, N, K, alpha, _ptr(A), lda, _ptr(B), ldb, beta, _ptr(Cm), ldc)
+
+
+def mygdrdgemm(m, n, k, alpha, a, na, b, nb, beta, c, nc) -> None:
+    lib().mygdrdgemm(m, n, k, alpha, _ptr(a), na, _ptr(b), nb, beta, _ptr(c), nc)
+
+
+def set_pivot_mode(mode: int) -> int:
+    return _check("lu2gpu_set_pivot_mode", lib().lu2gpu_set_pivot_mode(mode))
+
+
+# ---------------------------------------------------------------------------
+# device-resident API
+
+
+class Context:
+    """One lu2gpu context (a device, its stream and workspaces)."""
+
+    def __init__(self, device: int = 0):
+        self._h = C.c_void_p()
+        _check("lu2gpu_create", lib().lu2gpu_create(C.byref(self._h), device))
+        self.device = device
+
+    def close(self) -> None:
+        if self._h:
+            lib().lu2gpu_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_stream(self, stream) -> None:
+        """Run on an external cudaStream_t (e.g. torch.cuda.current_stream().cuda_stream)."""
+        _check("lu2gpu_set_stream", lib().lu2gpu_set_stream(self._h, int(stream)))
+
+    def generate(self, a, n: int, lda: int, seed: int, nrhs: int = 1, kind: int = 0) -> None:
+        """randomsetmat on the device (kind 1: diagonally dominant)."""
+        _check("lu2gpu_generate", lib().lu2gpu_generate(self._h, n, nrhs, seed, kind, _ptr(a), lda))
+
+    def factor(self, a, n: int, lda: int, nb: int, nrhs: int = 1, pivot_mode: int = PIVOT_PARTIAL,
+               ipiv=None) -> int:
+        return _check("lu2gpu_factor",
+                      lib().lu2gpu_factor(self._h, n, nrhs, _ptr(a), lda, nb, pivot_mode, _ptr(ipiv)))
+
+    def backsolve(self, a, n: int, lda: int, x, ldx: int, nrhs: int = 1) -> None:
+        _check("lu2gpu_backsolve", lib().lu2gpu_backsolve(self._h, n, nrhs, _ptr(a), lda, _ptr(x), ldx))
+
+    def lusolve(self, a, n: int, lda: int, nb: int, nrhs: int = 1, pivot_mode: int = PIVOT_PARTIAL,
+                ipiv=None) -> int:
+        """Factor + solve in place (x in columns n..n+nrhs-1)."""
+        return _check("lu2gpu_lusolve",
+                      lib().lu2gpu_lusolve(self._h, n, nrhs, _ptr(a), lda, nb, pivot_mode, _ptr(ipiv)))
+
+    def dgemm(self, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc) -> None:
+        _check("lu2gpu_dgemm_dev",
+               lib().lu2gpu_dgemm_dev(self._h, m, n, k, alpha, _ptr(a), lda, _ptr(b), ldb, beta, _ptr(c), ldc))
+
+    def pivots(self, n: int) -> np.ndarray:
+        out = np.zeros(n, dtype=np.int32)
+        _check("lu2gpu_copy_pivots", lib().lu2gpu_copy_pivots(self._h, _ptr(out), n))
+        return out
+
+    def set_timing(self, on: bool) -> None:
+        lib().lu2gpu_set_timing(self._h, 1 if on else 0)
+
+    def timers(self, reset: bool = True) -> dict:
+        ms = np.zeros(8, dtype=np.float64)
+        cnt = np.zeros(8, dtype=np.int64)
+        k = lib().lu2gpu_get_timers(self._h, _ptr(ms), _ptr(cnt), 8, 1 if reset else 0)
+        return {TIMER_NAMES[i]: (float(ms[i]), int(cnt[i])) for i in range(k)}
+
+
+def device_ld(n: int, nrhs: int = 1) -> int:
+    """A row stride for device matrices: >= n + nrhs, even, 128-byte rows."""
+    return ((n + nrhs + 15) // 16) * 16

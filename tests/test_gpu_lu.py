@@ -1,0 +1,180 @@
+"""Parity of the CUDA LU path (through the C ABI) with the oracle and with the
+reference's own results (golden vectors, and the compiled reference at
+n = 8192).
+
+Bars: pivots equal index for index; x within XTOL_PARTIAL (relative, max
+norm) of the fixed reference in partial-pivoting mode, and within XTOL_REF of
+the shipped reference in its bug-compatible mode (that algorithm amplifies
+rounding differences by its poor pivots); HPL scaled residual < 16 in
+partial-pivoting mode."""
+import numpy as np
+import pytest
+
+from lu2_b200 import PIVOT_PARTIAL, PIVOT_REF, device_ld, lumcolumn, rdim
+from oracle.oracle import RefLib
+
+pytestmark = pytest.mark.gpu
+
+XTOL_PARTIAL = 2e-11
+XTOL_REF = 1e-6
+GOLDEN_CASES = [(128, 64, 1), (256, 64, 12345), (512, 128, 12345), (1024, 256, 1), (2048, 64, 1),
+                (2048, 128, 12345), (2048, 256, 1)]
+
+
+def dev_matrix(ctx, n, seed, nrhs=1, kind=0):
+    import torch
+
+    ld = device_ld(n, nrhs)
+    a = torch.zeros((n, ld), dtype=torch.float64, device="cuda")
+    ctx.generate(a, n, ld, seed, nrhs, kind)
+    return a, ld
+
+
+def hpl(a0, x, n):
+    """||Ax-b||_inf / (eps (||A||_inf ||x||_inf + ||b||_inf) n), eps = 2^-53, in float64 on the host."""
+    A = a0[:, :n]
+    b = a0[:, n]
+    r = np.abs(A @ x - b).max()
+    return r / (2.0**-53 * (np.abs(A).sum(1).max() * np.abs(x).max() + np.abs(b).max()) * n)
+
+
+def test_generator_bit_exact(ctx, oracle):
+    n, nrhs = 301, 3
+    a, ld = dev_matrix(ctx, n, 12345, nrhs)
+    ref = oracle.randomsetmat(n, 12345, nrhs=nrhs)
+    assert np.array_equal(a.cpu().numpy()[:, : n + nrhs], ref[:, : n + nrhs])
+
+
+def test_generator_diagonally_dominant(ctx, oracle):
+    n = 200
+    a, ld = dev_matrix(ctx, n, 3, 1, kind=1)
+    g = a.cpu().numpy()
+    ref = oracle.randomsetmat(n, 3)
+    off = ~np.eye(n, dtype=bool)
+    assert np.array_equal(g[:, :n][off], ref[:, :n][off])
+    np.testing.assert_allclose(np.diag(g[:, :n]), np.abs(ref[:, :n]).sum(1), rtol=1e-13)
+
+
+@pytest.mark.parametrize("n,nb,seed", GOLDEN_CASES)
+@pytest.mark.parametrize("variant,mode,xtol", [("fixed", PIVOT_PARTIAL, XTOL_PARTIAL), ("shipped", PIVOT_REF, XTOL_REF)])
+def test_lusolve_matches_reference(ctx, golden, oracle, n, nb, seed, variant, mode, xtol):
+    a, ld = dev_matrix(ctx, n, seed)
+    info = ctx.lusolve(a, n, ld, nb, 1, mode)
+    assert info == 0
+    piv = ctx.pivots(n)
+    key = "%s_n%d_nb%d_s%d" % (variant, n, nb, seed)
+    np.testing.assert_array_equal(piv, golden[key + "_piv"])
+    x = a[:, n].cpu().numpy()
+    xr = golden[key + "_x"]
+    assert np.abs(x - xr).max() / np.abs(xr).max() < xtol
+    if mode == PIVOT_PARTIAL:
+        assert hpl(oracle.randomsetmat(n, seed), x, n) < 16
+
+
+def test_lumcolumn_host_entry(oracle):
+    n, nb, seed = 512, 64, 1
+    a = oracle.randomsetmat(n, seed)
+    b = np.zeros(n)
+    pv = np.zeros(nb, dtype=np.int32)
+    assert lumcolumn(a, b, nb, pv, PIVOT_PARTIAL) == 0
+    ao = oracle.randomsetmat(n, seed)
+    xo, po = oracle.lumcolumn(ao, n, nb, PIVOT_PARTIAL)
+    assert np.abs(b - xo).max() / np.abs(xo).max() < XTOL_PARTIAL
+    np.testing.assert_array_equal(pv, po[n - nb:])
+    # the factors land in the caller's array in lu2's storage (unit U', y in column n)
+    iu = np.triu_indices(n, 1)
+    assert np.abs(a[:, :n][iu] - ao[:, :n][iu]).max() < 1e-9
+    assert np.abs(a[:, n] - ao[:, n]).max() / np.abs(ao[:, n]).max() < 1e-10
+
+
+@pytest.mark.parametrize("n,nb", [(1, 16), (2, 16), (15, 16), (16, 16), (17, 16), (33, 16), (100, 32), (1000, 256),
+                                  (777, 64)])
+def test_ragged_sizes_vs_lapack(ctx, oracle, n, nb):
+    import scipy.linalg as sl
+
+    a, ld = dev_matrix(ctx, n, 11)
+    a0 = a.cpu().numpy().copy()
+    assert ctx.lusolve(a, n, ld, nb, 1, PIVOT_PARTIAL) == 0
+    lu, lp = sl.lu_factor(a0[:, :n])
+    np.testing.assert_array_equal(ctx.pivots(n), lp)
+    xs = sl.lu_solve((lu, lp), a0[:, n])
+    x = a[:, n].cpu().numpy()
+    assert np.abs(x - xs).max() / np.abs(xs).max() < 1e-10
+    assert hpl(a0, x, n) < 16
+
+
+def test_many_rhs(ctx):
+    import scipy.linalg as sl
+
+    n, nb, nrhs = 384, 64, 11
+    a, ld = dev_matrix(ctx, n, 5, nrhs)
+    a0 = a.cpu().numpy().copy()
+    assert ctx.lusolve(a, n, ld, nb, nrhs, PIVOT_PARTIAL) == 0
+    xs = sl.solve(a0[:, :n], a0[:, n:n + nrhs])
+    x = a[:, n:n + nrhs].cpu().numpy()
+    assert np.abs(x - xs).max() / np.abs(xs).max() < 1e-11
+
+
+def test_factor_then_separate_backsolve(ctx, oracle):
+    import torch
+
+    n, nb = 640, 128
+    a, ld = dev_matrix(ctx, n, 21)
+    a0 = a.cpu().numpy().copy()
+    ipiv = torch.zeros(n, dtype=torch.int32, device="cuda")
+    assert ctx.factor(a, n, ld, nb, 1, PIVOT_PARTIAL, ipiv) == 0
+    x = a[:, n].clone().reshape(n, 1).contiguous()
+    ctx.backsolve(a, n, ld, x, 1, 1)
+    assert hpl(a0, x.cpu().numpy()[:, 0], n) < 16
+    np.testing.assert_array_equal(ipiv.cpu().numpy(), ctx.pivots(n))
+
+
+def test_zero_pivot_reports_column(ctx):
+    import torch
+
+    n, nb = 96, 32
+    a, ld = dev_matrix(ctx, n, 2)
+    a[:, 40] = 0.0  # an exactly singular column
+    info = ctx.lusolve(a, n, ld, nb, 1, PIVOT_PARTIAL)
+    assert info == 41
+    assert torch.isfinite(a[:, :40]).all()
+
+
+def test_pivot_ties_go_to_lowest_row(ctx, oracle):
+    n, nb = 64, 16
+    a, ld = dev_matrix(ctx, n, 4)
+    a[:, 0] = 0.1
+    a[9, 0] = 0.5
+    a[5, 0] = -0.5  # same |a| as row 9, lower index
+    a0 = a.cpu().numpy().copy()
+    assert ctx.lusolve(a, n, ld, nb, 1, PIVOT_PARTIAL) == 0
+    assert ctx.pivots(n)[0] == 5
+    ao = np.zeros((n, n + 16))
+    ao[:, : n + 1] = a0[:, : n + 1]
+    _, po = oracle.lumcolumn(ao, n, nb, PIVOT_PARTIAL)
+    np.testing.assert_array_equal(ctx.pivots(n), po)
+
+
+@pytest.mark.skipif(not RefLib.available("fixed"), reason="compiled reference not present")
+@pytest.mark.parametrize("variant,mode", [("fixed", PIVOT_PARTIAL), ("shipped", PIVOT_REF)])
+def test_n8192_against_compiled_reference(ctx, oracle, variant, mode):
+    """configs[1]'s cross-check: the reference CPU lu2 at N=8192 on identical inputs."""
+    import os
+
+    n, nb, seed = 8192, 256, 1
+    ref = RefLib(variant)
+    ref.set_threads(max(1, min(32, os.cpu_count() or 1)), 1)
+    xr, pr, _ = ref.factor_solve(n, nb, seed)
+    a, ld = dev_matrix(ctx, n, seed)
+    assert ctx.lusolve(a, n, ld, nb, 1, mode) == 0
+    piv = ctx.pivots(n)
+    x = a[:, n].cpu().numpy()
+    rel = np.abs(x - xr).max() / np.abs(xr).max()
+    mism = int((piv != pr).sum())
+    print("n=8192 %s: pivot mismatches %d, x rel diff %.3e" % (variant, mism, rel))
+    assert mism == 0
+    if mode == PIVOT_PARTIAL:
+        assert rel < 1e-10
+        assert hpl(oracle.randomsetmat(n, seed), x, n) < 16
+    else:
+        assert rel < 1e-5
