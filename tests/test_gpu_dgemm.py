@@ -83,7 +83,7 @@ def test_mygdrdgemm_and_small_nk():
     c1 = c.copy()
     L.mygdrdgemm(m, n, k, -1.0, a, k, b, n, 1.0, c1, n)
     c2 = c.copy()
-    L.lib().matmul_for_small_nk(k, a.ctypes.data, n, b.ctypes.data, n, c2.ctypes.data, m, k, n)
+    L.load().matmul_for_small_nk(k, a.ctypes.data, n, b.ctypes.data, n, c2.ctypes.data, m, k, n)
     ref = c - a @ b
     assert np.all(np.abs(c1 - ref) <= bound(a, b, k, ref))
     assert np.array_equal(c1, c2)
@@ -94,7 +94,7 @@ def test_gdr_check_and_restart_selftest():
     a = np.zeros((N, N))
     b = np.zeros((N, N))
     c = np.zeros((N, N))
-    L.lib().gdr_check_and_restart(a.ctypes.data, b.ctypes.data, c.ctypes.data)
+    L.load().gdr_check_and_restart(a.ctypes.data, b.ctypes.data, c.ctypes.data)
     assert np.array_equal(c, b)
     assert b[5, 7] == 5 * N + 7
 
