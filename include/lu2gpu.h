@@ -179,6 +179,25 @@ const char *lu2gpu_timer_name(int phase);
 /* Number of CUDA kernels this library has launched in the process so far. */
 long lu2gpu_kernel_launches(void);
 
+/* lu2gpu_lusolve without any device allocation.  No counterpart in the
+ * reference: it exists for callers that cannot allocate device memory at the
+ * time they solve -- because another allocator already owns the device memory
+ * (a framework's caching allocator, a fixed memory budget), or because
+ * cudaMalloc/cudaFree would synchronize the whole device.  All scratch (pivot
+ * workspace, the transposed U block row, panel-exchange buffers, status words)
+ * comes from one fixed file-scope device array of about 2.1 MB that every GPU
+ * loading this library keeps until the process exits.  Limits: n <= 2048,
+ * 1 <= nrhs <= 16, 16 <= nb <= 128 (multiple of 16); larger sizes are
+ * rejected with LU2GPU_ERR_ARG.  a (device, lda even, 16-byte aligned) is
+ * factored and solved in place like lu2gpu_lusolve; ipiv (device, n ints) may
+ * be NULL.  Runs on `stream` (a cudaStream_t, NULL = the legacy default
+ * stream) on the current device and waits for it.  The first call on a device
+ * looks up the array's device address and the leaf kernel's launch limits for
+ * that device.  All calls share the one array, whose contents persist between
+ * calls: calls that overlap on the GPU (other streams, other host threads)
+ * race on it and must be serialized by the caller. */
+int lu2gpu_lusolve_noalloc(int n, int nrhs, double *a, long lda, int nb, int pivot_mode, int *ipiv, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

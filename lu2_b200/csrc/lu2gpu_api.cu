@@ -894,3 +894,117 @@ extern "C" int lu2gpu_copy_pivots(lu2gpu_ctx *c, int *ipiv_host, int n)
     CU_TRY(cudaMemcpy(ipiv_host, c->d_ipiv, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost));
     return 0;
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free solve for small systems.
+//
+// Some callers cannot allocate device memory when they need a solve: the
+// device memory may already be owned by another allocator (a framework's
+// caching allocator that has reserved most of HBM, or an application with a
+// fixed memory budget), or the caller cannot afford cudaMalloc/cudaFree, which
+// synchronize the whole device and stall every other stream.  For them this
+// entry point takes all of its scratch (pivot arrays, the transposed U block
+// row, the panel-exchange buffers, the status words) from one file-scope
+// device array of fixed size.  Every GPU that loads this library holds that
+// array until the process exits.
+
+constexpr int NOALLOC_MAX_N = 2048;
+constexpr int NOALLOC_MAX_NB = 128;
+constexpr int NOALLOC_MAX_NRHS = 16;
+constexpr int NOALLOC_LEAF_CTAS = (NOALLOC_MAX_N + 127) / 128;  // leaf grid at n <= 2048
+
+constexpr size_t na_round(size_t b) { return (b + 255) & ~size_t(255); }
+constexpr size_t NA_STATUS = 0;
+constexpr size_t NA_LEAF = NA_STATUS + na_round(4 * sizeof(int));
+constexpr size_t NA_LEAF_BYTES =
+    na_round((size_t)2 * NOALLOC_LEAF_CTAS * 16 * sizeof(double) + 2 * NOALLOC_LEAF_CTAS * sizeof(double) +
+             32 * sizeof(double) + 2 * NOALLOC_LEAF_CTAS * sizeof(int) + sizeof(unsigned));
+constexpr size_t NA_DINV = NA_LEAF + NA_LEAF_BYTES;
+constexpr size_t NA_IPIV = NA_DINV + na_round(NOALLOC_MAX_N * sizeof(double));
+constexpr size_t NA_BT = NA_IPIV + na_round(NOALLOC_MAX_N * sizeof(int));
+constexpr size_t NA_BT_BYTES =
+    ((size_t)(NOALLOC_MAX_N + NOALLOC_MAX_NRHS) * NOALLOC_MAX_NB + 1024) * sizeof(double);
+constexpr size_t NOALLOC_SCRATCH_BYTES = NA_BT + na_round(NA_BT_BYTES);  // about 2.1 MB
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+
+// Device address of g_noalloc_scratch per device, looked up once per device
+// with that device current.  In host code the symbol itself is only a host-side
+// stand-in and must never be passed to a kernel.
+static std::mutex g_noalloc_mu;
+static void *g_noalloc_ptr[128];
+static int g_noalloc_ctas[128];
+
+static int noalloc_setup(int device, unsigned char **base, int *leaf_ctas)
+{
+    if (device < 0 || device >= 128) {
+        set_error("lu2gpu_lusolve_noalloc: device ordinal %d out of range", device);
+        return LU2GPU_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[device]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            cudaGetLastError();
+            set_error("lu2gpu_lusolve_noalloc: cudaGetSymbolAddress failed on device %d: %s", device,
+                      cudaGetErrorString(e));
+            return LU2GPU_ERR_CUDA;
+        }
+        int ctas = leaf_max_ctas(device);
+        g_noalloc_ctas[device] = ctas < NOALLOC_LEAF_CTAS ? ctas : NOALLOC_LEAF_CTAS;
+        g_noalloc_ptr[device] = p;
+    }
+    *base = (unsigned char *)g_noalloc_ptr[device];
+    *leaf_ctas = g_noalloc_ctas[device];
+    return 0;
+}
+
+extern "C" int lu2gpu_lusolve_noalloc(int n, int nrhs, double *a, long lda, int nb, int pivot_mode, int *ipiv,
+                                      void *stream)
+{
+    if (n <= 0 || n > NOALLOC_MAX_N || nrhs < 1 || nrhs > NOALLOC_MAX_NRHS || nb > NOALLOC_MAX_NB) {
+        set_error("lu2gpu_lusolve_noalloc: n=%d nrhs=%d nb=%d outside the fixed scratch limits "
+                  "(n <= %d, 1 <= nrhs <= %d, nb <= %d)",
+                  n, nrhs, nb, NOALLOC_MAX_N, NOALLOC_MAX_NRHS, NOALLOC_MAX_NB);
+        return LU2GPU_ERR_ARG;
+    }
+    int rc = check_matrix_args(n, nrhs, a, lda, nb);
+    if (rc) return rc;
+    if (pivot_mode != LU2GPU_PIVOT_REF && pivot_mode != LU2GPU_PIVOT_PARTIAL) {
+        set_error("unknown pivot mode %d", pivot_mode);
+        return LU2GPU_ERR_ARG;
+    }
+    int device = 0;
+    CU_TRY(cudaGetDevice(&device));
+    unsigned char *base = nullptr;
+    int leaf_ctas = 0;
+    if ((rc = noalloc_setup(device, &base, &leaf_ctas))) return rc;
+
+    // A context on the host stack whose buffers all point into the scratch
+    // array; its capacities cover the limits above, so nothing is allocated.
+    lu2gpu_ctx c;
+    c.device = device;
+    c.stream = (cudaStream_t)stream;
+    c.own_stream = false;
+    c.d_status = (int *)(base + NA_STATUS);
+    c.leaf.xrow = (double *)(base + NA_LEAF);
+    c.leaf.xval = c.leaf.xrow + (size_t)2 * NOALLOC_LEAF_CTAS * 16;
+    c.leaf.rowc = c.leaf.xval + 2 * NOALLOC_LEAF_CTAS;
+    c.leaf.xidx = (int *)(c.leaf.rowc + 32);
+    c.leaf.bar = (unsigned *)(c.leaf.xidx + 2 * NOALLOC_LEAF_CTAS);
+    c.leaf_ctas = leaf_ctas;
+    c.d_dinv = (double *)(base + NA_DINV);
+    c.d_ipiv = ipiv ? ipiv : (int *)(base + NA_IPIV);
+    c.piv_cap = NOALLOC_MAX_N;
+    c.d_bt = (double *)(base + NA_BT);
+    c.bt_cap = NA_BT_BYTES;
+
+    // The status words must start cleared (begin_status); the leaf barrier
+    // counter is cleared before every leaf launch.  Pivots, 1/pivot and the U
+    // block row are written before they are read in every call.
+    if ((rc = begin_status(&c))) return rc;
+    if ((rc = factor_enqueue(&c, n, nrhs, a, lda, nb, pivot_mode))) return rc;
+    K_TRY(launch_backsolve(a, lda, n, nrhs, a + n, lda, c.stream));
+    return end_status(&c, "lu2gpu_lusolve_noalloc");
+}
