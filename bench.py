@@ -222,6 +222,8 @@ def main() -> int:
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="profiling run for ncu: generate the matrix and run exactly one factor+solve step")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -272,6 +274,16 @@ def main() -> int:
         info = ctx.lusolve(A, n, ld, nb, 1, L.PIVOT_PARTIAL)
         if info != 0:
             raise RuntimeError("zero pivot at column %d" % (info - 1))
+
+    if args.profile:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        step()
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_step_s": time.perf_counter() - t0, "n": n, "nb": nb,
+                          "launches": lib.lu2gpu_kernel_launches() - launches0}))
+        ctx.close()
+        return 0
 
     log("warmup x%d (n=%d nb=%d)" % (args.warmup, n, nb))
     for _ in range(args.warmup):

@@ -136,6 +136,16 @@ int lu2gpu_factor(lu2gpu_ctx *ctx, int n, int nrhs, double *a, long lda, int nb,
  * n x nrhs device block x (row stride ldx), overwritten by x. */
 int lu2gpu_backsolve(lu2gpu_ctx *ctx, int n, int nrhs, const double *a, long lda, double *x, long ldx);
 
+/* Solve A x = b again from the factors an earlier lu2gpu_factor left in a,
+ * with its pivot sequence ipiv (device) and its block size nb: the forward
+ * solve applies, panel by panel, exactly what the factorization applied to its
+ * augmented columns (pivots with 1/pivot scaling, unit-lower solve, update of
+ * the rows below; lu2.c:524-581), then the back substitution.  lu2 itself
+ * keeps only the last panel's pivots and cannot do this.  b (device, n x nrhs,
+ * row stride ldb) is overwritten by x.  a is not modified. */
+int lu2gpu_solve(lu2gpu_ctx *ctx, int n, const double *a, long lda, int nb, const int *ipiv, double *b, long ldb,
+                 int nrhs);
+
 /* lumcolumn on device memory: factor, then solve; x overwrites columns n..n+nrhs-1. */
 int lu2gpu_lusolve(lu2gpu_ctx *ctx, int n, int nrhs, double *a, long lda, int nb, int pivot_mode, int *ipiv);
 
@@ -169,8 +179,9 @@ int lu2gpu_set_abort_on_error(int on);
 const char *lu2gpu_last_error(void);
 
 /* Per-phase CUDA-event timers (the GPU counterpart of lu2's timerlib):
- * 0 "col dec t" panel, 1 "swaprows", 2 "solve tri", 3 "DGEMMrest" trailing
- * update, 4 "backward_sub".  get_timers fills ms[] and counts[] (launches)
+ * 0 "col dec t" panel leaves, 1 "swaprows", 2 "solve tri", 3 "DGEMMrest"
+ * trailing update, 4 "backward_sub", 5 "panel update" (the swaps, solves and
+ * updates inside the panel recursion).  get_timers fills ms[] and counts[] (launches)
  * for up to nmax phases, returns the number of phases. */
 int lu2gpu_set_timing(lu2gpu_ctx *ctx, int enable);
 int lu2gpu_get_timers(lu2gpu_ctx *ctx, double *ms, long *counts, int nmax, int reset);

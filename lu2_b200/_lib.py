@@ -46,6 +46,7 @@ SIGNATURES = {
     "lu2gpu_factor": (C.c_int, [vp, C.c_int, C.c_int, vp, C.c_long, C.c_int, C.c_int, vp]),
     "lu2gpu_backsolve": (C.c_int, [vp, C.c_int, C.c_int, vp, C.c_long, vp, C.c_long]),
     "lu2gpu_lusolve": (C.c_int, [vp, C.c_int, C.c_int, vp, C.c_long, C.c_int, C.c_int, vp]),
+    "lu2gpu_solve": (C.c_int, [vp, C.c_int, vp, C.c_long, C.c_int, vp, vp, C.c_long, C.c_int]),
     "lu2gpu_generate": (C.c_int, [vp, C.c_int, C.c_int, C.c_long, C.c_int, vp, C.c_long]),
     "lu2gpu_dgemm_dev": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_double, vp, C.c_long, vp, C.c_long,
                                    C.c_double, vp, C.c_long]),

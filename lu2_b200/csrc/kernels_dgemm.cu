@@ -12,6 +12,8 @@
 // k-permutation: the reduction index inside each 8-wide MMA step is permuted
 // consistently for A and B so that every thread's two k values are adjacent
 // in memory (one 16-byte shared load per fragment row).
+#include <cstdlib>
+
 #include "lu2gpu_internal.cuh"
 
 namespace lu2gpu {
@@ -117,12 +119,14 @@ struct GemmCfg {
     static constexpr int B_BYTES = BN * 128;
     static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
     static constexpr int SMEM = STAGES * STAGE_BYTES + 1024;
+    // 4-warp tiles are sized so that two CTAs share an SM
+    static constexpr int MINB = (THREADS <= 128) ? 2 : 1;
 };
 
 // MODE 0: C = C - A * Bt^T (accumulator starts from C, B fragments negated).
 // MODE 1: C = alpha * A * Bt^T + beta * C (C not read when beta == 0).
 template <int BM, int BN, int WM, int WN, int STAGES, int MODE>
-__global__ void __launch_bounds__(GemmCfg<BM, BN, WM, WN, STAGES>::THREADS)
+__global__ void __launch_bounds__(GemmCfg<BM, BN, WM, WN, STAGES>::THREADS, GemmCfg<BM, BN, WM, WN, STAGES>::MINB)
     dgemm_tn_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, GemmParams p)
 {
     using Cfg = GemmCfg<BM, BN, WM, WN, STAGES>;
@@ -161,9 +165,15 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, WM, WN, STAGES>::THREADS)
         for (int s = 0; s < STAGES && s < KT; s++) issue(s, s);
     }
 
+    // Fragment row g of every 8-row group is tile row pg = (g>>1) + 4(g&1), for
+    // A (M) and B (N) alike: the two rows a quarter-warp reads together are then
+    // r and r+4, which the 128-byte swizzle puts in opposite bank halves (rows g
+    // and g+1 would share the same 16 banks).  So accumulator c0 (MMA column 2t)
+    // is tile column t and c1 (2t+1) is tile column t+4.
+    const int pg = (g >> 1) + ((g & 1) << 2);
     double acc[MT][NT][4];
-    const int row_base = m0 + warp_m * WM + g;
-    const int col_base = n0 + warp_n * WN + 2 * t;
+    const int row_base = m0 + warp_m * WM + pg;
+    const int col_base = n0 + warp_n * WN + t;
 #pragma unroll
     for (int mt = 0; mt < MT; mt++)
 #pragma unroll
@@ -175,14 +185,8 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, WM, WN, STAGES>::THREADS)
                     const int m = row_base + mt * 16 + h * 8, n = col_base + nt * 8;
                     if (m < p.M) {
                         const double *cp = p.C + (size_t)m * p.ldc + n;
-                        if (p.vec_ok && n + 1 < p.N) {
-                            const double2 v = *reinterpret_cast<const double2 *>(cp);
-                            v0 = v.x;
-                            v1 = v.y;
-                        } else {
-                            if (n < p.N) v0 = cp[0];
-                            if (n + 1 < p.N) v1 = cp[1];
-                        }
+                        if (n < p.N) v0 = cp[0];
+                        if (n + 4 < p.N) v1 = cp[4];
                     }
                 }
                 acc[mt][nt][2 * h] = v0;
@@ -205,13 +209,13 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, WM, WN, STAGES>::THREADS)
             double bf[NT][2];
 #pragma unroll
             for (int nt = 0; nt < NT; nt++) {
-                const double2 v = lds_sw128(sb, warp_n * WN + nt * 8 + g, chunk);
+                const double2 v = lds_sw128(sb, warp_n * WN + nt * 8 + pg, chunk);
                 bf[nt][0] = (MODE == 0) ? -v.x : v.x;
                 bf[nt][1] = (MODE == 0) ? -v.y : v.y;
             }
 #pragma unroll
             for (int mt = 0; mt < MT; mt++) {
-                const int r = warp_m * WM + mt * 16 + g;
+                const int r = warp_m * WM + mt * 16 + pg;
                 const double2 lo = lds_sw128(sa, r, chunk);
                 const double2 hi = lds_sw128(sa, r + 8, chunk);
 #pragma unroll
@@ -233,21 +237,17 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, WM, WN, STAGES>::THREADS)
                 if (m >= p.M || n >= p.N) continue;
                 double *cp = p.C + (size_t)m * p.ldc + n;
                 double v0 = acc[mt][nt][2 * h], v1 = acc[mt][nt][2 * h + 1];
-                const bool two = n + 1 < p.N;
+                const bool two = n + 4 < p.N;
                 if (MODE == 1) {
                     v0 *= p.alpha;
                     v1 *= p.alpha;
                     if (p.beta != 0.0) {
                         v0 += p.beta * cp[0];
-                        if (two) v1 += p.beta * cp[1];
+                        if (two) v1 += p.beta * cp[4];
                     }
                 }
-                if (p.vec_ok && two) {
-                    *reinterpret_cast<double2 *>(cp) = make_double2(v0, v1);
-                } else {
-                    cp[0] = v0;
-                    if (two) cp[1] = v1;
-                }
+                cp[0] = v0;
+                if (two) cp[4] = v1;
             }
 }
 
@@ -311,7 +311,22 @@ static cudaError_t run_gemm(const CUtensorMap &ta, const CUtensorMap &tb, GemmPa
 // Tile shapes: wide trailing updates use 128x128 (8 warps of 64x32); narrow
 // right parts inside the panel recursion use 128x32.
 #define LU2_GEMM_WIDE 128, 128, 64, 32, 4
+#define LU2_GEMM_WIDE2 128, 64, 64, 32, 4
 #define LU2_GEMM_NARROW 128, 32, 32, 32, 4
+
+// wide tile shape: 1 = 128x64 with two CTAs per SM (default: one CTA's
+// prologue/epilogue overlaps the other's main loop; 89% of cuBLAS DGEMM at
+// N=32768 against 73% for 128x128), 0 = 128x128 with one CTA per SM.
+// LU2GPU_GEMM_WIDE=0 selects the latter (read once).
+static int wide_config()
+{
+    static int cfg = -1;
+    if (cfg < 0) {
+        const char *e = getenv("LU2GPU_GEMM_WIDE");
+        cfg = (e && e[0] == '0') ? 0 : 1;
+    }
+    return cfg;
+}
 
 // p.K is the loop extent (a multiple of 16); the maps' own extents
 // (a_cols, b_cols) bound what is read, the rest of a box reads as zero.
@@ -322,7 +337,8 @@ static cudaError_t gemm_dispatch(const double *a, long lda, long a_rows, long a_
     if (p.M <= 0 || p.N <= 0) return cudaSuccess;
     if (p.K <= 0 || (p.K & 15)) return cudaErrorInvalidValue;
     const bool narrow = p.N <= 64;
-    const int bm = 128, bn = narrow ? 32 : 128;
+    const int wide = wide_config();
+    const int bm = 128, bn = narrow ? 32 : (wide == 1 ? 64 : 128);
     CUtensorMap ta, tb;
     cudaError_t e = make_map(&ta, a, lda, a_rows, a_cols, bm);
     if (e != cudaSuccess) return e;
@@ -334,6 +350,7 @@ static cudaError_t gemm_dispatch(const double *a, long lda, long a_rows, long a_
     p.b_y0 = 0;
     p.vec_ok = ((reinterpret_cast<uintptr_t>(p.C) & 15) == 0 && (p.ldc & 1) == 0) ? 1 : 0;
     if (narrow) return run_gemm<LU2_GEMM_NARROW, MODE>(ta, tb, p, st);
+    if (wide == 1) return run_gemm<LU2_GEMM_WIDE2, MODE>(ta, tb, p, st);
     return run_gemm<LU2_GEMM_WIDE, MODE>(ta, tb, p, st);
 }
 

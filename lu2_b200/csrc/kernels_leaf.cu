@@ -1,0 +1,276 @@
+// kernels_leaf.cu -- the panel leaf: LU with partial pivoting of a slab of at
+// most 16 columns (rows c0..n-1), held in shared memory across one
+// cooperative grid.
+//
+// Reference behaviour (telmin/lu2): column_decomposition, lu2tlib.c:1041-1066,
+// inside the slab recursion lu2tlib.c:1095-1128 (16 -> 8 -> 4 -> 2); pivot
+// search cblas_idamax (first max of |a|), lu2tlib.c:42-52; the pivot row is
+// scaled by 1/pivot in every column but the diagonal, lu2tlib.c:1057-1059.
+// The leaf here runs the columns right-looking one by one, which is the same
+// elimination in a different order of operations.
+//
+// Per column the critical path is one exchange between CTAs: every CTA
+// publishes its candidate (largest |a| among its rows, its row values, and --
+// from the CTA owning row c -- row c itself) in a slot stamped with a 64-bit
+// sequence number (release store); every CTA polls all slots (acquire loads),
+// reduces them to the same winner, fetches the winner's row and updates its
+// own rows.  Each thread owns fixed slab rows, so the exchange, the swap, the
+// rank-1 update and the next column's local argmax need only two CTA barriers
+// per column.  Slots are double-buffered by column parity: a CTA can be at
+// most one column ahead of any other, because it needs every CTA's previous
+// publication to advance.
+#include <climits>
+
+#include "lu2gpu_internal.cuh"
+
+namespace lu2gpu {
+
+constexpr int LEAF_W = 16;            // widest leaf (lu2.c:1097: m <= 16)
+constexpr int LEAF_THREADS = 256;
+constexpr int LEAF_WARPS = LEAF_THREADS / 32;
+constexpr int LEAF_LDS = LEAF_W + 1;  // padded smem row
+constexpr int LEAF_MIN_ROWS = 128;    // rows per CTA below which fewer CTAs are used
+constexpr int LEAF_SMEM_MAX = 200 * 1024;
+
+struct LeafParams {
+    double *a;
+    long ld;
+    int n, c0, w, rows_per_cta, mode, goff;
+    int *ipiv;
+    double *dinv;
+    LeafSlot *slots;  // [2][gridDim.x]
+    unsigned long long seq0;
+    int *status;
+};
+
+__device__ __forceinline__ void st_release_u64(unsigned long long *p, unsigned long long v)
+{
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long *p)
+{
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__global__ void __launch_bounds__(LEAF_THREADS) leaf_kernel(LeafParams P)
+{
+    extern __shared__ double slab[];
+    // per-warp partial argmax: [0] the CTA's own candidate, [1] the global one
+    // (separate arrays: warp 0 may still read [0] while others fill [1])
+    __shared__ double s_wv[2][LEAF_WARPS];
+    __shared__ int s_wi[2][LEAF_WARPS];
+    __shared__ int s_fail;
+    const int G = gridDim.x, bid = blockIdx.x, tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const int w = P.w, c0 = P.c0, rpc = P.rows_per_cta;
+    const int rb = c0 + bid * rpc;
+    const int re = min(P.n, rb + rpc);
+    const int nr = max(0, re - rb);
+
+    for (int idx = tid; idx < nr * LEAF_W; idx += LEAF_THREADS) {
+        const int lr = idx / LEAF_W, j = idx - lr * LEAF_W;
+        slab[lr * LEAF_LDS + j] = (j < w) ? P.a[(size_t)(rb + lr) * P.ld + c0 + j] : 0.0;
+    }
+    if (tid == 0) s_fail = 0;
+    __syncthreads();
+
+    // search column of global column c (view column c0+ip)
+    auto search_col = [&](int ip) -> int {
+        const int c = c0 + ip;
+        if (P.mode == PIVOT_REF && ((c + P.goff) & 1) && ip > 0) return ip - 1;  // lu2tlib.c:1052
+        if (P.mode == PIVOT_REF_FIRST) return 0;
+        return ip;
+    };
+    // this thread's argmax over its own rows >= c in slab column sc
+    auto local_argmax = [&](int c, int sc, double &bv, int &bi) {
+        bv = -1.0;
+        bi = INT_MAX;
+        for (int lr = tid; lr < nr; lr += LEAF_THREADS) {
+            if (rb + lr < c) continue;
+            const double v = fabs(slab[lr * LEAF_LDS + sc]);
+            if (v > bv) {  // own rows visited in increasing order: keeps the first max
+                bv = v;
+                bi = rb + lr;
+            }
+        }
+    };
+
+    double bv;
+    int bi;
+    local_argmax(c0, search_col(0), bv, bi);
+
+    for (int ip = 0; ip < w; ip++) {
+        const int c = c0 + ip, par = ip & 1;
+        const unsigned long long seq = P.seq0 + (unsigned long long)ip + 1ull;
+        LeafSlot *myslot = P.slots + (size_t)par * G + bid;
+
+        // CTA candidate -> warp 0 publishes it (and row c, from its owner)
+        warp_argmax(bv, bi);
+        if (lane == 0) {
+            s_wv[0][warp] = bv;
+            s_wi[0][warp] = bi;
+        }
+        __syncthreads();  // S1
+        if (warp == 0) {
+            double v = lane < LEAF_WARPS ? s_wv[0][lane] : -1.0;
+            int i = lane < LEAF_WARPS ? s_wi[0][lane] : INT_MAX;
+            warp_argmax(v, i);
+            if (lane < LEAF_W) {
+                myslot->row[lane] = (i != INT_MAX) ? slab[(i - rb) * LEAF_LDS + lane] : 0.0;
+            } else if (c >= rb && c < re) {
+                myslot->rowc[lane - LEAF_W] = slab[(c - rb) * LEAF_LDS + lane - LEAF_W];
+            }
+            if (lane == 0) {
+                myslot->val = v;
+                myslot->idx = i;
+            }
+            __syncwarp();  // the lanes' slot writes precede lane 0's release store
+            if (lane == 0) st_release_u64(&myslot->seq, seq);
+        }
+
+        // warp 0 waits for every CTA's candidate of this column (relaxed polls,
+        // then one acquire fence) and reduces them to the winner
+        if (warp == 0) {
+            double gv = -1.0;
+            int gi = INT_MAX;
+            const unsigned long long t0 = globaltimer_ns();
+            bool failed = false;
+            for (int q = lane; q < G && !failed; q += 32) {
+                const unsigned long long *sq = &P.slots[(size_t)par * G + q].seq;
+                unsigned spins = 0;
+                while (ld_relaxed_u64(sq) != seq) {
+                    if ((++spins & 255u) == 0 &&
+                        (*(volatile int *)&P.status[1] != 0 || globaltimer_ns() - t0 > WAIT_LIMIT_NS)) {
+                        failed = true;
+                        break;
+                    }
+                }
+            }
+            if (__any_sync(0xffffffffu, failed)) {
+                if (lane == 0) {
+                    if (*(volatile int *)&P.status[1] == 0) record_error(P.status, ERR_BARRIER_TIMEOUT, 1);
+                    s_fail = 1;
+                }
+            } else {
+                asm volatile("fence.acq_rel.gpu;" ::: "memory");  // acquire side of the slots' release stores
+                for (int q = lane; q < G; q += 32) {
+                    const LeafSlot *s = P.slots + (size_t)par * G + q;
+                    const double v = __ldcg(&s->val);
+                    const int i = __ldcg(&s->idx);
+                    if (argmax_better(v, i, gv, gi)) {
+                        gv = v;
+                        gi = i;
+                    }
+                }
+                warp_argmax(gv, gi);
+                if (lane == 0) {
+                    s_wv[1][0] = gv;
+                    s_wi[1][0] = gi;
+                }
+            }
+        }
+        __syncthreads();  // S2
+        if (s_fail) break;
+        const double gv = s_wv[1][0];
+        const int gi = s_wi[1][0];
+        (void)gv;
+
+        const int p = (gi == INT_MAX) ? c : gi;  // no finite candidate (a NaN column): keep row c
+        const int owner_p = (p - c0) / rpc, owner_c = (c - c0) / rpc;
+        // lanes 0..15: the pivot row; lanes 16..31: old row c
+        double pr = 0.0;
+        if (lane < LEAF_W && lane < w)
+            pr = __ldcg(&P.slots[(size_t)par * G + owner_p].row[lane]);
+        else if (lane >= LEAF_W && lane - LEAF_W < w)
+            pr = __ldcg(&P.slots[(size_t)par * G + owner_c].rowc[lane - LEAF_W]);
+        const double d = __shfl_sync(0xffffffffu, pr, ip);
+        const bool zero = (d == 0.0);
+        const double inv = zero ? 1.0 : 1.0 / d;
+        double u[LEAF_W];   // scaled pivot row
+        double rc[LEAF_W];  // old row c (goes to row p)
+#pragma unroll
+        for (int j = 0; j < LEAF_W; j++) {
+            const double x = __shfl_sync(0xffffffffu, pr, j);
+            u[j] = (j == ip || zero) ? x : x * inv;
+            rc[j] = __shfl_sync(0xffffffffu, pr, LEAF_W + j);
+        }
+        if (bid == 0 && tid == 0) {
+            P.ipiv[c] = p + P.goff;
+            P.dinv[c] = inv;
+            if (zero) atomicMin(&P.status[0], c + 1);
+        }
+        // swap (by the threads owning rows c and p), then the rank-1 update of
+        // the own rows below c, then the own argmax for the next column
+        const int sc_next = (ip + 1 < w) ? search_col(ip + 1) : 0;
+        bv = -1.0;
+        bi = INT_MAX;
+        for (int lr = tid; lr < nr; lr += LEAF_THREADS) {
+            const int r = rb + lr;
+            if (r < c) continue;
+            double *row = slab + lr * LEAF_LDS;
+            if (r == c) {
+#pragma unroll
+                for (int j = 0; j < LEAF_W; j++) row[j] = u[j];
+                continue;
+            }
+            if (r == p) {
+#pragma unroll
+                for (int j = 0; j < LEAF_W; j++) row[j] = rc[j];
+            }
+            if (!zero) {
+                const double l = row[ip];
+#pragma unroll
+                for (int j = 0; j < LEAF_W; j++)
+                    if (j > ip && j < w) row[j] -= l * u[j];
+            }
+            if (ip + 1 < w) {
+                const double v = fabs(row[sc_next]);
+                if (v > bv) {
+                    bv = v;
+                    bi = r;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    for (int idx = tid; idx < nr * LEAF_W; idx += LEAF_THREADS) {
+        const int lr = idx / LEAF_W, j = idx - lr * LEAF_W;
+        if (j < w) P.a[(size_t)(rb + lr) * P.ld + c0 + j] = slab[lr * LEAF_LDS + j];
+    }
+}
+
+int leaf_max_ctas(int device)
+{
+    int sms = 0, per_sm = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    cudaFuncSetAttribute(leaf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, LEAF_SMEM_MAX);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, leaf_kernel, LEAF_THREADS, LEAF_SMEM_MAX);
+    if (per_sm < 1) per_sm = 1;
+    return sms * per_sm;
+}
+
+cudaError_t launch_leaf(double *a, long ld, int n, int c0, int w, int mode, int goff, int *ipiv, double *dinv,
+                        const LeafBuffers &buf, int *status, int max_ctas, cudaStream_t st)
+{
+    if (w <= 0) return cudaSuccess;
+    if (w > LEAF_W) return cudaErrorInvalidValue;
+    const int rows = n - c0;
+    int G = (rows + LEAF_MIN_ROWS - 1) / LEAF_MIN_ROWS;
+    if (G > max_ctas) G = max_ctas;
+    if (G > LEAF_THREADS) G = LEAF_THREADS;  // one polling thread per slot
+    if (G < 1) G = 1;
+    const int rpc = (rows + G - 1) / G;
+    G = (rows + rpc - 1) / rpc;
+    const size_t smem = (size_t)rpc * LEAF_LDS * sizeof(double);
+    if (smem > (size_t)LEAF_SMEM_MAX) return cudaErrorInvalidConfiguration;
+    LeafParams P{a, ld, n, c0, w, rpc, mode, goff, ipiv, dinv, buf.slots, *buf.seq, status};
+    *buf.seq += (unsigned long long)w;
+    void *args[] = {&P};
+    count_launch();
+    return cudaLaunchCooperativeKernel((const void *)leaf_kernel, dim3(G), dim3(LEAF_THREADS), args, smem, st);
+}
+
+}  // namespace lu2gpu

@@ -114,6 +114,24 @@ cudaError_t launch_backsolve(const double *a, long ld, int n, int nrhs, double *
     return cudaGetLastError();
 }
 
+// out[k] = 1 / a[k][k] (1 where the pivot is exactly zero), the same value the
+// leaf stored for the factorization's own 1/pivot scaling.
+__global__ void diag_inv_kernel(const double *a, long ld, int n, double *out)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const double d = a[(size_t)k * ld + k];
+    out[k] = (d == 0.0) ? 1.0 : 1.0 / d;
+}
+
+cudaError_t launch_diag_inv(const double *a, long ld, int n, double *out, cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    count_launch();
+    diag_inv_kernel<<<(n + 255) / 256, 256, 0, st>>>(a, ld, n, out);
+    return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------------------
 // drand48 stream
 

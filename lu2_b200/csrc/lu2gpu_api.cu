@@ -57,8 +57,10 @@ static void fail_void(const char *where)
 // ---------------------------------------------------------------------------
 // context
 
-enum { PH_PANEL = 0, PH_SWAP, PH_TRSM, PH_DGEMM, PH_BACKSOLVE, PH_COUNT };
-static const char *g_phase_names[PH_COUNT] = {"col dec t", "swaprows", "solve tri", "DGEMMrest", "backward_sub"};
+// phase 0 is the panel leaves, 5 the updates inside the panel recursion
+enum { PH_LEAF = 0, PH_SWAP, PH_TRSM, PH_DGEMM, PH_BACKSOLVE, PH_PANEL, PH_COUNT };
+static const char *g_phase_names[PH_COUNT] = {"col dec t",    "swaprows",    "solve tri",
+                                              "DGEMMrest",    "backward_sub", "panel update"};
 
 struct lu2gpu_ctx {
     int device = 0;
@@ -71,6 +73,7 @@ struct lu2gpu_ctx {
     double *d_dinv = nullptr;
     size_t piv_cap = 0;
     LeafBuffers leaf{};
+    unsigned long long leaf_seq = 0;  // leaf publication stamps issued so far
     int leaf_ctas = 0;
     int leaf_w = 16;
     // staging for the host-pointer entry points
@@ -79,8 +82,8 @@ struct lu2gpu_ctx {
     // phase timers
     bool timing = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[PH_COUNT];
-    double acc_ms[PH_COUNT] = {0, 0, 0, 0, 0};
-    long launches[PH_COUNT] = {0, 0, 0, 0, 0};
+    double acc_ms[PH_COUNT] = {};
+    long launches[PH_COUNT] = {};
 };
 
 struct DeviceGuard {
@@ -156,20 +159,17 @@ extern "C" int lu2gpu_create(lu2gpu_ctx **out, int device)
     c->own_stream = true;
     c->leaf_ctas = leaf_max_ctas(device);
     const int G = c->leaf_ctas;
-    size_t leaf_bytes = (size_t)2 * G * 16 * sizeof(double) + 2 * G * sizeof(double) + 2 * G * sizeof(int) +
-                        2 * 16 * sizeof(double) + 256;
+    size_t leaf_bytes = (size_t)2 * G * sizeof(LeafSlot);
     char *lb = nullptr;
-    if (cudaMalloc(&c->d_status, 4 * sizeof(int)) != cudaSuccess || cudaMalloc(&lb, leaf_bytes) != cudaSuccess) {
+    if (cudaMalloc(&c->d_status, 4 * sizeof(int)) != cudaSuccess || cudaMalloc(&lb, leaf_bytes) != cudaSuccess ||
+        cudaMemset(lb, 0, leaf_bytes) != cudaSuccess) {
         cudaGetLastError();
         set_error("cudaMalloc of the context buffers failed");
         lu2gpu_destroy(c);
         return LU2GPU_ERR_NOMEM;
     }
-    c->leaf.xrow = (double *)lb;
-    c->leaf.xval = c->leaf.xrow + (size_t)2 * G * 16;
-    c->leaf.rowc = c->leaf.xval + 2 * G;
-    c->leaf.xidx = (int *)(c->leaf.rowc + 32);
-    c->leaf.bar = (unsigned *)(c->leaf.xidx + 2 * G);
+    c->leaf.slots = (LeafSlot *)lb;
+    c->leaf.seq = &c->leaf_seq;
     *out = c;
     return 0;
 }
@@ -180,7 +180,7 @@ extern "C" int lu2gpu_destroy(lu2gpu_ctx *c)
     DeviceGuard g(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     cudaFree(c->d_status);
-    cudaFree(c->leaf.xrow);
+    cudaFree(c->leaf.slots);
     cudaFree(c->d_bt);
     cudaFree(c->d_ipiv);
     cudaFree(c->d_dinv);
@@ -358,7 +358,7 @@ static int right_part(lu2gpu_ctx *c, const View &v, int k0, int k1, int cs, int 
 static int panel(lu2gpu_ctx *c, const View &v, int c0, int m, int mode)
 {
     if (m <= c->leaf_w) {
-        PhaseTimer t(c, PH_PANEL);
+        PhaseTimer t(c, PH_LEAF);
         K_TRY(launch_leaf(v.a, v.ld, v.n, c0, m, mode, v.goff, c->d_ipiv + v.goff, c->d_dinv + v.goff, c->leaf,
                           c->d_status, c->leaf_ctas, c->stream));
         return 0;
@@ -515,6 +515,42 @@ extern "C" int lu2gpu_lusolve(lu2gpu_ctx *c, int n, int nrhs, double *a, long ld
     }
     if (ipiv) CU_TRY(cudaMemcpyAsync(ipiv, c->d_ipiv, (size_t)n * sizeof(int), cudaMemcpyDeviceToDevice, c->stream));
     return end_status(c, "lu2gpu_lusolve");
+}
+
+// Solve with the factors of an earlier lu2gpu_factor: per panel of width nb
+// (the factorization's, so that the panel's L columns are read in the row
+// order they were stored in), the panel's pivots with the 1/pivot scaling, the
+// unit-lower solve and the update of the rows below -- what the factorization
+// does to its augmented columns (lu2.c:524-581) -- then the back substitution
+// (lu2.c:110-116).  b (n x nrhs, row stride ldb) is overwritten by x.
+extern "C" int lu2gpu_solve(lu2gpu_ctx *c, int n, const double *a, long lda, int nb, const int *ipiv, double *b,
+                            long ldb, int nrhs)
+{
+    if (!c || n <= 0 || !a || lda < n || !ipiv || !b || nrhs < 1 || ldb < nrhs) {
+        set_error("lu2gpu_solve: bad arguments");
+        return LU2GPU_ERR_ARG;
+    }
+    int rc = check_matrix_args(n, 0, a, lda, nb);
+    if (rc) return rc;
+    if (nb > NB_MAX) nb = NB_MAX;
+    DeviceGuard g(c->device);
+    if ((rc = ensure_work(c, n, nrhs, nb))) return rc;
+    if ((rc = begin_status(c))) return rc;
+    K_TRY(launch_diag_inv(a, lda, n, c->d_dinv, c->stream));
+    for (int i = 0; i < n; i += nb) {
+        const int w = (n - i) < nb ? (n - i) : nb;
+        K_TRY(launch_laswp_scale(b, ldb, i, i + w, ipiv, 0, c->d_dinv, 0, nrhs, true, c->stream));
+        K_TRY(launch_trsm_unit_lower_tx(a + (size_t)i * lda + i, lda, b + (size_t)i * ldb, ldb, w, nrhs, c->d_bt,
+                                        c->stream));
+        if (i + w < n)
+            K_TRY(launch_dgemm_update(a, lda, n, i + w, i, c->d_bt, b + (size_t)(i + w) * ldb, ldb, n - i - w, nrhs,
+                                      w, c->d_status, c->stream));
+    }
+    {
+        PhaseTimer t(c, PH_BACKSOLVE);
+        K_TRY(launch_backsolve(a, lda, n, nrhs, b, ldb, c->stream));
+    }
+    return end_status(c, "lu2gpu_solve");
 }
 
 extern "C" int lu2gpu_generate(lu2gpu_ctx *c, int n, int nrhs, long seed, int kind, double *a, long lda)
@@ -916,9 +952,7 @@ constexpr int NOALLOC_LEAF_CTAS = (NOALLOC_MAX_N + 127) / 128;  // leaf grid at 
 constexpr size_t na_round(size_t b) { return (b + 255) & ~size_t(255); }
 constexpr size_t NA_STATUS = 0;
 constexpr size_t NA_LEAF = NA_STATUS + na_round(4 * sizeof(int));
-constexpr size_t NA_LEAF_BYTES =
-    na_round((size_t)2 * NOALLOC_LEAF_CTAS * 16 * sizeof(double) + 2 * NOALLOC_LEAF_CTAS * sizeof(double) +
-             32 * sizeof(double) + 2 * NOALLOC_LEAF_CTAS * sizeof(int) + sizeof(unsigned));
+constexpr size_t NA_LEAF_BYTES = na_round((size_t)2 * NOALLOC_LEAF_CTAS * sizeof(LeafSlot));
 constexpr size_t NA_DINV = NA_LEAF + NA_LEAF_BYTES;
 constexpr size_t NA_IPIV = NA_DINV + na_round(NOALLOC_MAX_N * sizeof(double));
 constexpr size_t NA_BT = NA_IPIV + na_round(NOALLOC_MAX_N * sizeof(int));
@@ -934,6 +968,9 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH
 static std::mutex g_noalloc_mu;
 static void *g_noalloc_ptr[128];
 static int g_noalloc_ctas[128];
+// leaf publication stamps per device; the slots start zeroed (static storage)
+// and every stamp is used once, so leftovers of earlier calls never match
+static unsigned long long g_noalloc_seq[128];
 
 static int noalloc_setup(int device, unsigned char **base, int *leaf_ctas)
 {
@@ -988,11 +1025,8 @@ extern "C" int lu2gpu_lusolve_noalloc(int n, int nrhs, double *a, long lda, int 
     c.stream = (cudaStream_t)stream;
     c.own_stream = false;
     c.d_status = (int *)(base + NA_STATUS);
-    c.leaf.xrow = (double *)(base + NA_LEAF);
-    c.leaf.xval = c.leaf.xrow + (size_t)2 * NOALLOC_LEAF_CTAS * 16;
-    c.leaf.rowc = c.leaf.xval + 2 * NOALLOC_LEAF_CTAS;
-    c.leaf.xidx = (int *)(c.leaf.rowc + 32);
-    c.leaf.bar = (unsigned *)(c.leaf.xidx + 2 * NOALLOC_LEAF_CTAS);
+    c.leaf.slots = (LeafSlot *)(base + NA_LEAF);
+    c.leaf.seq = &g_noalloc_seq[device];
     c.leaf_ctas = leaf_ctas;
     c.d_dinv = (double *)(base + NA_DINV);
     c.d_ipiv = ipiv ? ipiv : (int *)(base + NA_IPIV);

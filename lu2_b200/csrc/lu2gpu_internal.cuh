@@ -70,12 +70,19 @@ __device__ __forceinline__ void warp_argmax(double &v, int &i)
 // process-wide count of this library's kernel launches (lu2gpu_kernel_launches)
 void count_launch(long k = 1);
 
+// One CTA's published pivot candidate for one leaf column.
+struct __align__(64) LeafSlot {
+    double row[16];          // the candidate row's leaf columns
+    double rowc[16];         // row c (written by the CTA owning row c only)
+    double val;              // |a| of the candidate in the search column
+    int idx;                 // its row (view numbering), INT_MAX if none
+    int pad_;
+    unsigned long long seq;  // publication stamp (release store)
+};
+
 struct LeafBuffers {
-    double *xrow;   // [2][maxG][16]
-    double *xval;   // [2][maxG]
-    int *xidx;      // [2][maxG]
-    double *rowc;   // [2][16]
-    unsigned *bar;  // grid barrier counter
+    LeafSlot *slots;          // [2][max CTAs], zeroed once
+    unsigned long long *seq;  // host-side stamp counter, advanced by every leaf launch
 };
 
 // Factor the leaf panel: rows c0..n-1, columns c0..c0+w-1 (w <= 16) of the
@@ -95,6 +102,10 @@ cudaError_t launch_laswp_scale(double *a, long ld, int k0, int k1, const int *ip
 // a[r0..r0+K)[r0..r0+K) and X = a[r0..r0+K)[cs..ce); also writes
 // bt[(j-cs)*K + l] = X[l][j] (the transposed block row for the update GEMM).
 cudaError_t launch_trsm_unit_lower(double *a, long ld, int r0, int K, int cs, int ce, double *bt, cudaStream_t st);
+// The same with the triangle T (row stride ldt) and the K x ncols block X
+// (row stride ldx) given separately; bt may be null.
+cudaError_t launch_trsm_unit_lower_tx(const double *t, long ldt, double *x, long ldx, int K, int ncols, double *bt,
+                                      cudaStream_t st);
 
 // C[m][n] -= sum_k A[m][k] * Bt[n][k], the trailing update.  A is the
 // row-major matrix starting at (a_row0, a_col0) of `a` (stride ld, rows < a_rows
@@ -114,6 +125,9 @@ cudaError_t launch_transpose(const double *in, long ldi, double *out, long ldo, 
 // lu2.c:110-116); y (n x nrhs, row stride ldx) is overwritten by x.  For lu2's
 // own layout x = a + n, ldx = ld.
 cudaError_t launch_backsolve(const double *a, long ld, int n, int nrhs, double *x, long ldx, cudaStream_t st);
+
+// out[k] = 1 / a[k][k] (1 for an exactly zero pivot)
+cudaError_t launch_diag_inv(const double *a, long ld, int n, double *out, cudaStream_t st);
 
 // lu2's matrix generator (randomsetmat, lu2.c:70-85) on the device, bit-identical to
 // glibc drand48: row i holds draws i*(n+1) .. i*(n+1)+n (b_i last); extra

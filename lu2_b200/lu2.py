@@ -20,7 +20,7 @@ from . import _lib
 PIVOT_REF = 0
 PIVOT_PARTIAL = 1
 CBLAS_ROWMAJOR, CBLAS_COLMAJOR, CBLAS_NOTRANS, CBLAS_TRANS = 101, 102, 111, 112
-TIMER_NAMES = ["col dec t", "swaprows", "solve tri", "DGEMMrest", "backward_sub"]
+TIMER_NAMES = ["col dec t", "swaprows", "solve tri", "DGEMMrest", "backward_sub", "panel update"]
 
 
 class Lu2GpuError(RuntimeError):
@@ -157,6 +157,10 @@ class Context:
         """Factor + solve in place (x in columns n..n+nrhs-1)."""
         return _check("lu2gpu_lusolve",
                       lib().lu2gpu_lusolve(self._h, n, nrhs, _ptr(a), lda, nb, pivot_mode, _ptr(ipiv)))
+
+    def solve(self, a, n: int, lda: int, nb: int, ipiv, b, ldb: int, nrhs: int = 1) -> None:
+        """Re-solve from stored factors (device a, ipiv) into b (overwritten by x)."""
+        _check("lu2gpu_solve", lib().lu2gpu_solve(self._h, n, _ptr(a), lda, nb, _ptr(ipiv), _ptr(b), ldb, nrhs))
 
     def dgemm(self, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc) -> None:
         _check("lu2gpu_dgemm_dev",

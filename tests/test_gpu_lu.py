@@ -129,6 +129,38 @@ def test_factor_then_separate_backsolve(ctx, oracle):
     np.testing.assert_array_equal(ipiv.cpu().numpy(), ctx.pivots(n))
 
 
+@pytest.mark.parametrize("mode", [PIVOT_PARTIAL, PIVOT_REF])
+def test_resolve_from_stored_factors(ctx, mode):
+    """lu2gpu_solve: new right-hand sides against the stored factors (lu2's
+    storage + the full pivot sequence), including one factored with nrhs = 0."""
+    import scipy.linalg as sl
+    import torch
+
+    n, nb = 1000, 64
+    a, ld = dev_matrix(ctx, n, 31)
+    a0 = a.cpu().numpy().copy()
+    ipiv = torch.zeros(n, dtype=torch.int32, device="cuda")
+    assert ctx.factor(a, n, ld, nb, 1, mode, ipiv) == 0
+    x_aug = a[:, n].clone().reshape(n, 1).contiguous()
+    ctx.backsolve(a, n, ld, x_aug, 1, 1)
+    rng = np.random.default_rng(0)
+    B = np.concatenate([a0[:, n:n + 1], rng.uniform(-0.5, 0.5, (n, 2))], axis=1)
+    b = torch.tensor(B, device="cuda").contiguous()
+    ctx.solve(a, n, ld, nb, ipiv, b, 3, 3)
+    xs = sl.solve(a0[:, :n], B)
+    xb = b.cpu().numpy()
+    tol = 1e-10 if mode == PIVOT_PARTIAL else 1e-6
+    assert np.abs(xb - xs).max() / np.abs(xs).max() < tol
+    xa = x_aug.cpu().numpy()[:, 0]
+    assert np.abs(xb[:, 0] - xa).max() / np.abs(xa).max() < 1e-13
+    # factor without a riding right-hand side, then solve
+    a2, _ = dev_matrix(ctx, n, 31)
+    assert ctx.factor(a2, n, ld, nb, 0, mode, ipiv) == 0
+    b2 = torch.tensor(B[:, :1], device="cuda").contiguous()
+    ctx.solve(a2, n, ld, nb, ipiv, b2, 1, 1)
+    assert np.abs(b2.cpu().numpy()[:, 0] - xa).max() / np.abs(xa).max() < 1e-13
+
+
 def test_zero_pivot_reports_column(ctx):
     import torch
 
