@@ -45,6 +45,7 @@ extern "C" {
 #define LU2GPU_ERR_NOMEM (-3)
 #define LU2GPU_ERR_TIMEOUT (-4) /* a bounded device wait gave up */
 #define LU2GPU_ERR_NODEV (-5)
+#define LU2GPU_ERR_NOCONV (-6) /* iterative refinement did not reach its residual bound */
 
 /* pivot search */
 #define LU2GPU_PIVOT_REF 0     /* bug-compatible with lu2tlib.c:1052 (see below) */
@@ -155,6 +156,29 @@ int lu2gpu_lusolve(lu2gpu_ctx *ctx, int n, int nrhs, double *a, long lda, int nb
  * kind 0: as lu2; kind 1: then a_ii = sum_j |a_ij| over the row (diagonally
  * dominant).  nrhs >= 1. */
 int lu2gpu_generate(lu2gpu_ctx *ctx, int n, int nrhs, long seed, int kind, double *a, long lda);
+
+/* Precision form (no counterpart in the reference, whose solver is FP64
+ * only): solve A x = b for the FP64 n x n device matrix a (lda even, a
+ * 16-byte aligned, not modified) by lu2's factorization of an FP32 copy --
+ * the panel in FP32, the trailing updates as BF16 tensor-core products with
+ * FP32 accumulation and per-panel power-of-two operand scales, block size nb
+ * in {64, 128, 192, 256} -- followed by classical iterative refinement with
+ * the residual r = b - A x and the update of x in FP64, until the HPL scaled
+ * residual ||r||/(eps (||A|| ||x|| + ||b||) n) (inf-norms, eps = 2^-53) is
+ * below 16 or max_iter corrections were applied.  b, x: device n-vectors.
+ * out (host, may be NULL) receives {iterations, final scaled residual,
+ * factorization seconds, refinement seconds}.  Returns 0 when the bound was
+ * met, LU2GPU_ERR_NOCONV when not, > 0 on a zero pivot, < 0 on errors. */
+int lu2gpu_mixed_solve(lu2gpu_ctx *ctx, int n, const double *a, long lda, const double *b, double *x, int nb,
+                       int pivot_mode, int max_iter, double *out);
+
+/* The precision form's trailing update on its own (the BF16 counterpart of
+ * mmmulandsub, lu2.c:312-343): c (FP32, M x N, row stride ldc) -= scale *
+ * a * bt^T with a (M x K) and bt (N x K) BF16 device matrices, K-contiguous
+ * (row strides lda, ldb multiples of 8, 16-byte aligned), K in {64, 128,
+ * 192, 256}; tcgen05 tensor cores with FP32 accumulation. */
+int lu2gpu_bf16_update_dev(lu2gpu_ctx *ctx, int M, int N, int K, const void *a, long lda, const void *bt, long ldb,
+                           float *c, long ldc, float scale);
 
 /* Row-major device DGEMM, C = alpha*A*B + beta*C (mydgemm's contract). */
 int lu2gpu_dgemm_dev(lu2gpu_ctx *ctx, int m, int n, int k, double alpha, const double *a, long lda, const double *b,

@@ -47,6 +47,9 @@ SIGNATURES = {
     "lu2gpu_backsolve": (C.c_int, [vp, C.c_int, C.c_int, vp, C.c_long, vp, C.c_long]),
     "lu2gpu_lusolve": (C.c_int, [vp, C.c_int, C.c_int, vp, C.c_long, C.c_int, C.c_int, vp]),
     "lu2gpu_solve": (C.c_int, [vp, C.c_int, vp, C.c_long, C.c_int, vp, vp, C.c_long, C.c_int]),
+    "lu2gpu_mixed_solve": (C.c_int, [vp, C.c_int, vp, C.c_long, vp, vp, C.c_int, C.c_int, C.c_int, vp]),
+    "lu2gpu_bf16_update_dev": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, vp, C.c_long, vp, C.c_long, vp, C.c_long,
+                                         C.c_float]),
     "lu2gpu_generate": (C.c_int, [vp, C.c_int, C.c_int, C.c_long, C.c_int, vp, C.c_long]),
     "lu2gpu_dgemm_dev": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_double, vp, C.c_long, vp, C.c_long,
                                    C.c_double, vp, C.c_long]),

@@ -32,12 +32,13 @@ constexpr int LEAF_LDS = LEAF_W + 1;  // padded smem row
 constexpr int LEAF_MIN_ROWS = 128;    // rows per CTA below which fewer CTAs are used
 constexpr int LEAF_SMEM_MAX = 200 * 1024;
 
+template <typename T>
 struct LeafParams {
-    double *a;
+    T *a;
     long ld;
     int n, c0, w, rows_per_cta, mode, goff;
     int *ipiv;
-    double *dinv;
+    T *dinv;
     LeafSlot *slots;  // [2][gridDim.x]
     unsigned long long seq0;
     int *status;
@@ -55,9 +56,13 @@ __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long
     return v;
 }
 
-__global__ void __launch_bounds__(LEAF_THREADS) leaf_kernel(LeafParams P)
+// T = double (plain form) or float (the precision form's FP32 panel); the
+// exchanged candidate rows are carried as double, which holds either exactly.
+template <typename T>
+__global__ void __launch_bounds__(LEAF_THREADS) leaf_kernel(LeafParams<T> P)
 {
-    extern __shared__ double slab[];
+    extern __shared__ __align__(16) unsigned char leaf_smem[];
+    T *slab = reinterpret_cast<T *>(leaf_smem);
     // per-warp partial argmax: [0] the CTA's own candidate, [1] the global one
     // (separate arrays: warp 0 may still read [0] while others fill [1])
     __shared__ double s_wv[2][LEAF_WARPS];
@@ -186,16 +191,16 @@ __global__ void __launch_bounds__(LEAF_THREADS) leaf_kernel(LeafParams P)
             pr = __ldcg(&P.slots[(size_t)par * G + owner_p].row[lane]);
         else if (lane >= LEAF_W && lane - LEAF_W < w)
             pr = __ldcg(&P.slots[(size_t)par * G + owner_c].rowc[lane - LEAF_W]);
-        const double d = __shfl_sync(0xffffffffu, pr, ip);
-        const bool zero = (d == 0.0);
-        const double inv = zero ? 1.0 : 1.0 / d;
-        double u[LEAF_W];   // scaled pivot row
-        double rc[LEAF_W];  // old row c (goes to row p)
+        const T d = (T)__shfl_sync(0xffffffffu, pr, ip);
+        const bool zero = (d == T(0));
+        const T inv = zero ? T(1) : T(1) / d;
+        T u[LEAF_W];   // scaled pivot row
+        T rc[LEAF_W];  // old row c (goes to row p)
 #pragma unroll
         for (int j = 0; j < LEAF_W; j++) {
-            const double x = __shfl_sync(0xffffffffu, pr, j);
+            const T x = (T)__shfl_sync(0xffffffffu, pr, j);
             u[j] = (j == ip || zero) ? x : x * inv;
-            rc[j] = __shfl_sync(0xffffffffu, pr, LEAF_W + j);
+            rc[j] = (T)__shfl_sync(0xffffffffu, pr, LEAF_W + j);
         }
         if (bid == 0 && tid == 0) {
             P.ipiv[c] = p + P.goff;
@@ -210,7 +215,7 @@ __global__ void __launch_bounds__(LEAF_THREADS) leaf_kernel(LeafParams P)
         for (int lr = tid; lr < nr; lr += LEAF_THREADS) {
             const int r = rb + lr;
             if (r < c) continue;
-            double *row = slab + lr * LEAF_LDS;
+            T *row = slab + lr * LEAF_LDS;
             if (r == c) {
 #pragma unroll
                 for (int j = 0; j < LEAF_W; j++) row[j] = u[j];
@@ -221,7 +226,7 @@ __global__ void __launch_bounds__(LEAF_THREADS) leaf_kernel(LeafParams P)
                 for (int j = 0; j < LEAF_W; j++) row[j] = rc[j];
             }
             if (!zero) {
-                const double l = row[ip];
+                const T l = row[ip];
 #pragma unroll
                 for (int j = 0; j < LEAF_W; j++)
                     if (j > ip && j < w) row[j] -= l * u[j];
@@ -246,14 +251,16 @@ int leaf_max_ctas(int device)
 {
     int sms = 0, per_sm = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    cudaFuncSetAttribute(leaf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, LEAF_SMEM_MAX);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, leaf_kernel, LEAF_THREADS, LEAF_SMEM_MAX);
+    cudaFuncSetAttribute(leaf_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, LEAF_SMEM_MAX);
+    cudaFuncSetAttribute(leaf_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, LEAF_SMEM_MAX);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, leaf_kernel<double>, LEAF_THREADS, LEAF_SMEM_MAX);
     if (per_sm < 1) per_sm = 1;
     return sms * per_sm;
 }
 
-cudaError_t launch_leaf(double *a, long ld, int n, int c0, int w, int mode, int goff, int *ipiv, double *dinv,
-                        const LeafBuffers &buf, int *status, int max_ctas, cudaStream_t st)
+template <typename T>
+static cudaError_t launch_leaf_t(T *a, long ld, int n, int c0, int w, int mode, int goff, int *ipiv, T *dinv,
+                                 const LeafBuffers &buf, int *status, int max_ctas, cudaStream_t st)
 {
     if (w <= 0) return cudaSuccess;
     if (w > LEAF_W) return cudaErrorInvalidValue;
@@ -264,13 +271,25 @@ cudaError_t launch_leaf(double *a, long ld, int n, int c0, int w, int mode, int 
     if (G < 1) G = 1;
     const int rpc = (rows + G - 1) / G;
     G = (rows + rpc - 1) / rpc;
-    const size_t smem = (size_t)rpc * LEAF_LDS * sizeof(double);
+    const size_t smem = (size_t)rpc * LEAF_LDS * sizeof(T);
     if (smem > (size_t)LEAF_SMEM_MAX) return cudaErrorInvalidConfiguration;
-    LeafParams P{a, ld, n, c0, w, rpc, mode, goff, ipiv, dinv, buf.slots, *buf.seq, status};
+    LeafParams<T> P{a, ld, n, c0, w, rpc, mode, goff, ipiv, dinv, buf.slots, *buf.seq, status};
     *buf.seq += (unsigned long long)w;
     void *args[] = {&P};
     count_launch();
-    return cudaLaunchCooperativeKernel((const void *)leaf_kernel, dim3(G), dim3(LEAF_THREADS), args, smem, st);
+    return cudaLaunchCooperativeKernel((const void *)leaf_kernel<T>, dim3(G), dim3(LEAF_THREADS), args, smem, st);
+}
+
+cudaError_t launch_leaf(double *a, long ld, int n, int c0, int w, int mode, int goff, int *ipiv, double *dinv,
+                        const LeafBuffers &buf, int *status, int max_ctas, cudaStream_t st)
+{
+    return launch_leaf_t(a, ld, n, c0, w, mode, goff, ipiv, dinv, buf, status, max_ctas, st);
+}
+
+cudaError_t launch_leaf(float *a, long ld, int n, int c0, int w, int mode, int goff, int *ipiv, float *dinv,
+                        const LeafBuffers &buf, int *status, int max_ctas, cudaStream_t st)
+{
+    return launch_leaf_t(a, ld, n, c0, w, mode, goff, ipiv, dinv, buf, status, max_ctas, st);
 }
 
 }  // namespace lu2gpu

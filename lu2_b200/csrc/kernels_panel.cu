@@ -8,6 +8,8 @@
 //   trsm        lu2.c:485-521 (solve_triangle: U12 = L11^{-1} A12)
 #include <climits>
 
+#include <cuda_bf16.h>
+
 #include "lu2gpu_internal.cuh"
 
 namespace lu2gpu {
@@ -27,9 +29,10 @@ namespace lu2gpu {
 constexpr int SWAP_COLS = 16;
 constexpr int SWAP_THREADS = 256;
 
-__global__ void __launch_bounds__(SWAP_THREADS) laswp_scale_kernel(double *a, long ld, int k0, int k1,
+template <typename T>
+__global__ void __launch_bounds__(SWAP_THREADS) laswp_scale_kernel(T *a, long ld, int k0, int k1,
                                                                    const int *__restrict__ ipiv, int goff,
-                                                                   const double *__restrict__ dinv, int cs, int ce,
+                                                                   const T *__restrict__ dinv, int cs, int ce,
                                                                    int scale)
 {
     extern __shared__ int sw[];
@@ -40,7 +43,7 @@ __global__ void __launch_bounds__(SWAP_THREADS) laswp_scale_kernel(double *a, lo
     int *cur = slot + npiv;       // [2 npiv] slot content
     int *rowof = cur + 2 * npiv;  // [2 npiv] row of each slot
     __shared__ int s_nslot;
-    double *V = reinterpret_cast<double *>(sw + ((7 * npiv + 1) & ~1));  // [2 npiv][SWAP_COLS], 8-byte aligned
+    T *V = reinterpret_cast<T *>(sw + ((7 * npiv + 1) & ~1));  // [2 npiv][SWAP_COLS], 8-byte aligned
     const int tid = threadIdx.x;
 
     for (int t = tid; t < npiv; t += SWAP_THREADS) {
@@ -97,7 +100,7 @@ __global__ void __launch_bounds__(SWAP_THREADS) laswp_scale_kernel(double *a, lo
         __syncthreads();
         if (jok) {
             for (int s = tid / SWAP_COLS; s < nslot; s += SWAP_THREADS / SWAP_COLS) {
-                double v = V[s * SWAP_COLS + c];
+                T v = V[s * SWAP_COLS + c];
                 if (scale && s < npiv) v *= __ldg(dinv + k0 + s);
                 a[(size_t)rowof[s] * ld + j] = v;
             }
@@ -106,16 +109,17 @@ __global__ void __launch_bounds__(SWAP_THREADS) laswp_scale_kernel(double *a, lo
     }
 }
 
-cudaError_t launch_laswp_scale(double *a, long ld, int k0, int k1, const int *ipiv, int goff, const double *dinv,
-                               int cs, int ce, bool scale, cudaStream_t st)
+template <typename T>
+static cudaError_t launch_laswp_scale_t(T *a, long ld, int k0, int k1, const int *ipiv, int goff, const T *dinv,
+                                        int cs, int ce, bool scale, cudaStream_t st)
 {
     if (ce <= cs || k1 <= k0) return cudaSuccess;
     const int npiv = k1 - k0;
-    const size_t smem = (size_t)7 * npiv * sizeof(int) + 8 + (size_t)2 * npiv * SWAP_COLS * sizeof(double);
+    const size_t smem = (size_t)7 * npiv * sizeof(int) + 8 + (size_t)2 * npiv * SWAP_COLS * sizeof(T);
     if (smem > 200 * 1024) return cudaErrorInvalidValue;
     if (smem > 48 * 1024) {
         cudaError_t e =
-            cudaFuncSetAttribute(laswp_scale_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            cudaFuncSetAttribute(laswp_scale_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         if (e != cudaSuccess) return e;
     }
     // the permutation is built once per CTA; CTAs then stride over 16-column chunks
@@ -125,8 +129,20 @@ cudaError_t launch_laswp_scale(double *a, long ld, int k0, int k1, const int *ip
     int blocks = (ce - cs + SWAP_COLS - 1) / SWAP_COLS;
     if (blocks > 3 * sms) blocks = 3 * sms;
     count_launch();
-    laswp_scale_kernel<<<blocks, SWAP_THREADS, smem, st>>>(a, ld, k0, k1, ipiv, goff, dinv, cs, ce, scale ? 1 : 0);
+    laswp_scale_kernel<T><<<blocks, SWAP_THREADS, smem, st>>>(a, ld, k0, k1, ipiv, goff, dinv, cs, ce, scale ? 1 : 0);
     return cudaGetLastError();
+}
+
+cudaError_t launch_laswp_scale(double *a, long ld, int k0, int k1, const int *ipiv, int goff, const double *dinv,
+                               int cs, int ce, bool scale, cudaStream_t st)
+{
+    return launch_laswp_scale_t(a, ld, k0, k1, ipiv, goff, dinv, cs, ce, scale, st);
+}
+
+cudaError_t launch_laswp_scale(float *a, long ld, int k0, int k1, const int *ipiv, int goff, const float *dinv,
+                               int cs, int ce, bool scale, cudaStream_t st)
+{
+    return launch_laswp_scale_t(a, ld, k0, k1, ipiv, goff, dinv, cs, ce, scale, st);
 }
 
 // ---------------------------------------------------------------------------
@@ -141,12 +157,15 @@ constexpr int TRSM_BK = 16;
 constexpr int TRSM_TLD = TRSM_BK + 1;
 
 // T: the unit lower triangle (strict lower part used), row stride ldt; X: the
-// K x ncols block (row stride ldx) solved in place; bt (optional) receives X^T.
-__global__ void __launch_bounds__(256) trsm_unit_lower_kernel(const double *T, long ldt, double *Xg, long ldx, int K,
-                                                              int ncols, double *bt)
+// K x ncols block (row stride ldx) solved in place; bt (optional) receives
+// X^T * bt_scale converted to BT (double, float or bf16).
+template <typename E, typename BT>
+__global__ void __launch_bounds__(256) trsm_unit_lower_kernel(const E *T, long ldt, E *Xg, long ldx, int K, int ncols,
+                                                              BT *bt, const float *bt_scale)
 {
-    extern __shared__ double X[];  // K x TRSM_LDS, then Ts: K x TRSM_TLD
-    double *Ts = X + (size_t)K * TRSM_LDS;
+    extern __shared__ __align__(16) unsigned char trsm_smem[];
+    E *X = reinterpret_cast<E *>(trsm_smem);  // K x TRSM_LDS, then Ts: K x TRSM_TLD
+    E *Ts = X + (size_t)K * TRSM_LDS;
     const int col = threadIdx.x & 31, rg = threadIdx.x >> 5;
     const int j = blockIdx.x * TRSM_TW + col;
     const bool jok = j < ncols;
@@ -161,16 +180,16 @@ __global__ void __launch_bounds__(256) trsm_unit_lower_kernel(const double *T, l
         }
         __syncthreads();
         for (int l = 0; l + 1 < bk; l++) {
-            const double xl = X[(lb + l) * TRSM_LDS + col];
+            const E xl = X[(lb + l) * TRSM_LDS + col];
             for (int r = l + 1 + rg; r < bk; r += 8) X[(lb + r) * TRSM_LDS + col] -= Ts[r * TRSM_TLD + l] * xl;
             __syncthreads();
         }
-        double xb[TRSM_BK];
+        E xb[TRSM_BK];
 #pragma unroll
         for (int l = 0; l < TRSM_BK; l++) xb[l] = (l < bk) ? X[(lb + l) * TRSM_LDS + col] : 0.0;
         for (int r = lb + bk + rg; r < K; r += 8) {
-            const double *Tr = Ts + (r - lb) * TRSM_TLD;
-            double s = 0.0;
+            const E *Tr = Ts + (r - lb) * TRSM_TLD;
+            E s = 0;
 #pragma unroll
             for (int l = 0; l < TRSM_BK; l++) s += Tr[l] * xb[l];
             X[r * TRSM_LDS + col] -= s;
@@ -180,33 +199,56 @@ __global__ void __launch_bounds__(256) trsm_unit_lower_kernel(const double *T, l
     for (int r = rg; r < K; r += 8)
         if (jok) Xg[(size_t)r * ldx + j] = X[r * TRSM_LDS + col];
     if (!bt) return;
+    const float sc = bt_scale ? *bt_scale : 1.0f;
     const int jbase = blockIdx.x * TRSM_TW;
     for (int idx = threadIdx.x; idx < TRSM_TW * K; idx += 256) {
         const int cc = idx / K, r = idx - cc * K;
-        if (jbase + cc < ncols) bt[(size_t)(jbase + cc) * K + r] = X[r * TRSM_LDS + cc];
+        if (jbase + cc < ncols) {
+            const E v = X[r * TRSM_LDS + cc];
+            bt[(size_t)(jbase + cc) * K + r] = bt_scale ? (BT)(float)(v * (E)sc) : (BT)v;
+        }
     }
+}
+
+template <typename E, typename BT>
+static cudaError_t launch_trsm_t(const E *t, long ldt, E *x, long ldx, int K, int ncols, BT *bt, const float *bt_scale,
+                                 cudaStream_t st)
+{
+    if (ncols <= 0 || K <= 0) return cudaSuccess;
+    const size_t smem = (size_t)K * (TRSM_LDS + TRSM_TLD) * sizeof(E);
+    if (smem > 210 * 1024) return cudaErrorInvalidValue;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(trsm_unit_lower_kernel<E, BT>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, 210 * 1024);
+        if (e != cudaSuccess) return e;
+    }
+    const int blocks = (ncols + TRSM_TW - 1) / TRSM_TW;
+    count_launch();
+    trsm_unit_lower_kernel<E, BT><<<blocks, 256, smem, st>>>(t, ldt, x, ldx, K, ncols, bt, bt_scale);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_trsm_unit_lower_tx(const double *t, long ldt, double *x, long ldx, int K, int ncols, double *bt,
                                       cudaStream_t st)
 {
-    if (ncols <= 0 || K <= 0) return cudaSuccess;
-    const size_t smem = (size_t)K * (TRSM_LDS + TRSM_TLD) * sizeof(double);
-    if (smem > 210 * 1024) return cudaErrorInvalidValue;
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(trsm_unit_lower_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             210 * 1024);
-        if (e != cudaSuccess) return e;
-    }
-    const int blocks = (ncols + TRSM_TW - 1) / TRSM_TW;
-    count_launch();
-    trsm_unit_lower_kernel<<<blocks, 256, smem, st>>>(t, ldt, x, ldx, K, ncols, bt);
-    return cudaGetLastError();
+    return launch_trsm_t<double, double>(t, ldt, x, ldx, K, ncols, bt, nullptr, st);
 }
 
 cudaError_t launch_trsm_unit_lower(double *a, long ld, int r0, int K, int cs, int ce, double *bt, cudaStream_t st)
 {
     return launch_trsm_unit_lower_tx(a + (size_t)r0 * ld + r0, ld, a + (size_t)r0 * ld + cs, ld, K, ce - cs, bt, st);
+}
+
+cudaError_t launch_trsm_unit_lower_f32(const float *t, long ldt, float *x, long ldx, int K, int ncols, float *bt,
+                                       cudaStream_t st)
+{
+    return launch_trsm_t<float, float>(t, ldt, x, ldx, K, ncols, bt, nullptr, st);
+}
+
+cudaError_t launch_trsm_unit_lower_f32_bf16(const float *t, long ldt, float *x, long ldx, int K, int ncols, void *bt,
+                                            const float *bt_scale, cudaStream_t st)
+{
+    return launch_trsm_t<float, __nv_bfloat16>(t, ldt, x, ldx, K, ncols, (__nv_bfloat16 *)bt, bt_scale, st);
 }
 
 }  // namespace lu2gpu

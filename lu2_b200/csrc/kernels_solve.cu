@@ -19,11 +19,13 @@ constexpr int BS_MAXR = 8;  // right-hand sides handled per pass
 
 // Solve the unit upper diagonal block rows r0..r0+bs-1 for columns
 // n+c0..n+c0+nr-1 (nr <= BS_MAXR).  One CTA.
-__global__ void __launch_bounds__(256) backsolve_diag_kernel(const double *a, long ld, int r0, int bs, double *x,
-                                                             long ldx, int c0, int nr)
+template <typename T>
+__global__ void __launch_bounds__(256) backsolve_diag_kernel(const T *a, long ld, int r0, int bs, T *x, long ldx,
+                                                             int c0, int nr)
 {
-    extern __shared__ double U[];  // bs x (bs+1)
-    __shared__ double X[BS_BLOCK][BS_MAXR];
+    extern __shared__ __align__(16) unsigned char bs_smem[];
+    T *U = reinterpret_cast<T *>(bs_smem);  // bs x (bs+1)
+    __shared__ T X[BS_BLOCK][BS_MAXR];
     const int lds = bs + 1;
     for (int idx = threadIdx.x; idx < bs * bs; idx += blockDim.x) {
         const int r = idx / bs, c = idx - r * bs;
@@ -37,7 +39,7 @@ __global__ void __launch_bounds__(256) backsolve_diag_kernel(const double *a, lo
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int c = warp; c < nr; c += blockDim.x >> 5) {
         for (int j = bs - 1; j >= 0; j--) {
-            double s = 0.0;
+            T s = 0;
             for (int k = j + 1 + lane; k < bs; k += 32) s += U[j * lds + k] * X[k][c];
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
@@ -53,10 +55,11 @@ __global__ void __launch_bounds__(256) backsolve_diag_kernel(const double *a, lo
 }
 
 // y[i][c] -= sum_{k in block} U'[i][k] x[k][c] for rows i < r0; one warp per row.
-__global__ void __launch_bounds__(256) backsolve_update_kernel(const double *a, long ld, int r0, int bs, double *x,
-                                                               long ldx, int c0, int nr)
+template <typename T>
+__global__ void __launch_bounds__(256) backsolve_update_kernel(const T *a, long ld, int r0, int bs, T *x, long ldx,
+                                                               int c0, int nr)
 {
-    __shared__ double X[BS_BLOCK][BS_MAXR];
+    __shared__ T X[BS_BLOCK][BS_MAXR];
     for (int idx = threadIdx.x; idx < bs * nr; idx += blockDim.x) {
         const int r = idx / nr, c = idx - r * nr;
         X[r][c] = x[(size_t)(r0 + r) * ldx + c0 + c];
@@ -65,12 +68,12 @@ __global__ void __launch_bounds__(256) backsolve_update_kernel(const double *a, 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int wpb = blockDim.x >> 5;
     for (int i = blockIdx.x * wpb + warp; i < r0; i += gridDim.x * wpb) {
-        const double *row = a + (size_t)i * ld + r0;
-        double s[BS_MAXR];
+        const T *row = a + (size_t)i * ld + r0;
+        T s[BS_MAXR];
 #pragma unroll
-        for (int c = 0; c < BS_MAXR; c++) s[c] = 0.0;
+        for (int c = 0; c < BS_MAXR; c++) s[c] = 0;
         for (int k = lane; k < bs; k += 32) {
-            const double u = __ldcs(row + k);
+            const T u = __ldcs(row + k);
 #pragma unroll
             for (int c = 0; c < BS_MAXR; c++)
                 if (c < nr) s[c] += u * X[k][c];
@@ -78,7 +81,7 @@ __global__ void __launch_bounds__(256) backsolve_update_kernel(const double *a, 
 #pragma unroll
         for (int c = 0; c < BS_MAXR; c++) {
             if (c >= nr) break;
-            double v = s[c];
+            T v = s[c];
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
             if (lane == 0) x[(size_t)i * ldx + c0 + c] -= v;
@@ -86,10 +89,11 @@ __global__ void __launch_bounds__(256) backsolve_update_kernel(const double *a, 
     }
 }
 
-cudaError_t launch_backsolve(const double *a, long ld, int n, int nrhs, double *x, long ldx, cudaStream_t st)
+template <typename T>
+static cudaError_t launch_backsolve_t(const T *a, long ld, int n, int nrhs, T *x, long ldx, cudaStream_t st)
 {
-    cudaError_t e = cudaFuncSetAttribute(backsolve_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         BS_BLOCK * (BS_BLOCK + 1) * (int)sizeof(double));
+    cudaError_t e = cudaFuncSetAttribute(backsolve_diag_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         BS_BLOCK * (BS_BLOCK + 1) * (int)sizeof(T));
     if (e != cudaSuccess) return e;
     int sms = 148, dev = 0;
     cudaGetDevice(&dev);
@@ -100,35 +104,54 @@ cudaError_t launch_backsolve(const double *a, long ld, int n, int nrhs, double *
         for (int b = nblk - 1; b >= 0; b--) {
             const int r0 = b * BS_BLOCK;
             const int bs = (n - r0) < BS_BLOCK ? (n - r0) : BS_BLOCK;
-            const size_t smem = (size_t)bs * (bs + 1) * sizeof(double);
+            const size_t smem = (size_t)bs * (bs + 1) * sizeof(T);
             count_launch();
-            backsolve_diag_kernel<<<1, 256, smem, st>>>(a, ld, r0, bs, x, ldx, c0, nr);
+            backsolve_diag_kernel<T><<<1, 256, smem, st>>>(a, ld, r0, bs, x, ldx, c0, nr);
             if (r0 > 0) {
                 int blocks = (r0 + 7) / 8;
                 if (blocks > sms * 8) blocks = sms * 8;
                 count_launch();
-                backsolve_update_kernel<<<blocks, 256, 0, st>>>(a, ld, r0, bs, x, ldx, c0, nr);
+                backsolve_update_kernel<T><<<blocks, 256, 0, st>>>(a, ld, r0, bs, x, ldx, c0, nr);
             }
         }
     }
     return cudaGetLastError();
 }
 
+cudaError_t launch_backsolve(const double *a, long ld, int n, int nrhs, double *x, long ldx, cudaStream_t st)
+{
+    return launch_backsolve_t(a, ld, n, nrhs, x, ldx, st);
+}
+
+cudaError_t launch_backsolve(const float *a, long ld, int n, int nrhs, float *x, long ldx, cudaStream_t st)
+{
+    return launch_backsolve_t(a, ld, n, nrhs, x, ldx, st);
+}
+
 // out[k] = 1 / a[k][k] (1 where the pivot is exactly zero), the same value the
 // leaf stored for the factorization's own 1/pivot scaling.
-__global__ void diag_inv_kernel(const double *a, long ld, int n, double *out)
+template <typename T>
+__global__ void diag_inv_kernel(const T *a, long ld, int n, T *out)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
-    const double d = a[(size_t)k * ld + k];
-    out[k] = (d == 0.0) ? 1.0 : 1.0 / d;
+    const T d = a[(size_t)k * ld + k];
+    out[k] = (d == T(0)) ? T(1) : T(1) / d;
 }
 
 cudaError_t launch_diag_inv(const double *a, long ld, int n, double *out, cudaStream_t st)
 {
     if (n <= 0) return cudaSuccess;
     count_launch();
-    diag_inv_kernel<<<(n + 255) / 256, 256, 0, st>>>(a, ld, n, out);
+    diag_inv_kernel<double><<<(n + 255) / 256, 256, 0, st>>>(a, ld, n, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_diag_inv(const float *a, long ld, int n, float *out, cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    count_launch();
+    diag_inv_kernel<float><<<(n + 255) / 256, 256, 0, st>>>(a, ld, n, out);
     return cudaGetLastError();
 }
 

@@ -84,7 +84,11 @@ struct lu2gpu_ctx {
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[PH_COUNT];
     double acc_ms[PH_COUNT] = {};
     long launches[PH_COUNT] = {};
+    // workspaces of the precision form (lu2gpu_mixed_solve), allocated on first use
+    struct MixedWork *mx = nullptr;
 };
+
+static void free_mixed(lu2gpu_ctx *c);
 
 struct DeviceGuard {
     int prev = -1;
@@ -185,6 +189,7 @@ extern "C" int lu2gpu_destroy(lu2gpu_ctx *c)
     cudaFree(c->d_ipiv);
     cudaFree(c->d_dinv);
     for (int i = 0; i < 4; i++) cudaFree(c->d_stage[i]);
+    free_mixed(c);
     for (int p = 0; p < PH_COUNT; p++)
         for (auto &e : c->ev[p]) {
             cudaEventDestroy(e.first);
@@ -1041,4 +1046,258 @@ extern "C" int lu2gpu_lusolve_noalloc(int n, int nrhs, double *a, long lda, int 
     if ((rc = factor_enqueue(&c, n, nrhs, a, lda, nb, pivot_mode))) return rc;
     K_TRY(launch_backsolve(a, lda, n, nrhs, a + n, lda, c.stream));
     return end_status(&c, "lu2gpu_lusolve_noalloc");
+}
+
+// ---------------------------------------------------------------------------
+// Precision form: lu2's factorization (same recursion, pivoting and storage)
+// on an FP32 copy of A, the panel in exact FP32, the trailing updates as BF16
+// products on the tensor cores with FP32 accumulation and per-panel
+// power-of-two operand scales; then classical iterative refinement with the
+// residual r = b - A x and the update of x in FP64 until the HPL scaled
+// residual is below 16.
+
+struct MixedWork {
+    float *a32 = nullptr;
+    size_t a32_cap = 0;
+    void *l16 = nullptr;  // L21 of the current panel, BF16, M x nb
+    size_t l16_cap = 0;
+    void *u16 = nullptr;  // U12 transposed, BF16, N x nb
+    size_t u16_cap = 0;
+    float *bt32 = nullptr;  // transposed U blocks of the panel recursion (FP32)
+    size_t bt32_cap = 0;
+    float *dinv = nullptr;
+    size_t dinv_cap = 0;
+    double *vec = nullptr;  // x, r, rowabs (n doubles each) + v32 (n floats)
+    size_t vec_cap = 0;
+    void *small = nullptr;  // amax[2] (float bits), scales[3], norms[4] (double bits)
+    size_t small_cap = 0;
+    unsigned *amax() { return (unsigned *)small; }
+    float *scales() { return (float *)((char *)small + 16); }
+    unsigned long long *norms() { return (unsigned long long *)((char *)small + 64); }
+};
+
+static void free_mixed(lu2gpu_ctx *c)
+{
+    if (!c->mx) return;
+    MixedWork *m = c->mx;
+    cudaFree(m->a32);
+    cudaFree(m->l16);
+    cudaFree(m->u16);
+    cudaFree(m->bt32);
+    cudaFree(m->dinv);
+    cudaFree(m->vec);
+    cudaFree(m->small);
+    delete m;
+    c->mx = nullptr;
+}
+
+static int mixed_work(lu2gpu_ctx *c, int n, long ld32, int nb)
+{
+    if (!c->mx) c->mx = new MixedWork();
+    MixedWork *m = c->mx;
+    int rc;
+    if ((rc = grow((void **)&m->a32, &m->a32_cap, (size_t)n * ld32 * sizeof(float)))) return rc;
+    if ((rc = grow(&m->l16, &m->l16_cap, (size_t)n * nb * 2 + 1024))) return rc;
+    if ((rc = grow(&m->u16, &m->u16_cap, (size_t)n * nb * 2 + 1024))) return rc;
+    if ((rc = grow((void **)&m->bt32, &m->bt32_cap, (size_t)nb * nb * sizeof(float) + 1024))) return rc;
+    if ((rc = grow((void **)&m->dinv, &m->dinv_cap, (size_t)n * sizeof(float) + 256))) return rc;
+    if ((rc = grow((void **)&m->vec, &m->vec_cap, (size_t)n * (3 * sizeof(double) + sizeof(float)) + 1024))) return rc;
+    if ((rc = grow(&m->small, &m->small_cap, 256))) return rc;
+    return ensure_work(c, n, 16, nb);  // pivot sequence in c->d_ipiv
+}
+
+struct View32 {
+    float *a;
+    long ld;
+    int n, ncols, goff;
+};
+
+static int right_part32(lu2gpu_ctx *c, const View32 &v, int k0, int k1, int cs, int ce, bool top)
+{
+    if (ce <= cs) return 0;
+    MixedWork *m = c->mx;
+    int *ipiv = c->d_ipiv + v.goff;
+    float *dinv = m->dinv + v.goff;
+    const int K = k1 - k0;
+    {
+        PhaseTimer t(c, top ? PH_SWAP : PH_PANEL);
+        K_TRY(launch_laswp_scale(v.a, v.ld, k0, k1, ipiv, v.goff, dinv, cs, ce, true, c->stream));
+    }
+    const float *T = v.a + (size_t)k0 * v.ld + k0;
+    float *X = v.a + (size_t)k0 * v.ld + cs;
+    if (!top) {
+        PhaseTimer t(c, PH_PANEL);
+        K_TRY(launch_trsm_unit_lower_f32(T, v.ld, X, v.ld, K, ce - cs, m->bt32, c->stream));
+        if (k1 < v.n)
+            K_TRY(launch_sgemm_update(v.a + (size_t)k1 * v.ld + k0, v.ld, m->bt32, v.a + (size_t)k1 * v.ld + cs, v.ld,
+                                      v.n - k1, ce - cs, K, c->stream));
+        return 0;
+    }
+    {
+        PhaseTimer t(c, PH_TRSM);
+        K_TRY(launch_trsm_unit_lower_f32(T, v.ld, X, v.ld, K, ce - cs, nullptr, c->stream));
+    }
+    if (k1 < v.n) {
+        PhaseTimer t(c, PH_DGEMM);
+        const int M = v.n - k1, N = ce - cs;
+        const float *L = v.a + (size_t)k1 * v.ld + k0;
+        CU_TRY(cudaMemsetAsync(m->amax(), 0, 2 * sizeof(unsigned), c->stream));
+        K_TRY(launch_absmax(L, v.ld, M, K, m->amax(), c->stream));
+        K_TRY(launch_absmax(X, v.ld, K, N, m->amax() + 1, c->stream));
+        K_TRY(launch_panel_scales(m->amax(), m->scales(), c->stream));
+        K_TRY(launch_f32_to_bf16(L, v.ld, m->l16, K, M, K, m->scales(), c->stream));
+        K_TRY(launch_f32_transpose_bf16(X, v.ld, K, N, m->u16, m->scales() + 1, c->stream));
+        K_TRY(launch_bf16_update(m->l16, K, m->u16, K, v.a + (size_t)k1 * v.ld + cs, v.ld, M, N, K, m->scales() + 2,
+                                 c->d_status, c->stream));
+    }
+    return 0;
+}
+
+static int panel32(lu2gpu_ctx *c, const View32 &v, int c0, int m, int mode)
+{
+    if (m <= c->leaf_w) {
+        PhaseTimer t(c, PH_LEAF);
+        K_TRY(launch_leaf(v.a, v.ld, v.n, c0, m, mode, v.goff, c->d_ipiv + v.goff, c->mx->dinv + v.goff, c->leaf,
+                          c->d_status, c->leaf_ctas, c->stream));
+        return 0;
+    }
+    int h = ((m / 2) + 15) & ~15;
+    if (h >= m) h = m - 16;
+    int rc = panel32(c, v, c0, h, mode);
+    if (rc) return rc;
+    if ((rc = right_part32(c, v, c0, c0 + h, c0 + h, c0 + m, false))) return rc;
+    if ((rc = panel32(c, v, c0 + h, m - h, mode))) return rc;
+    PhaseTimer t(c, PH_PANEL);
+    K_TRY(launch_laswp_scale(v.a, v.ld, c0 + h, c0 + m, c->d_ipiv + v.goff, v.goff, c->mx->dinv + v.goff, c0, c0 + h,
+                             true, c->stream));
+    return 0;
+}
+
+// FP32 forward solve with the stored factors (what the factorization applies
+// to an augmented column, panel by panel), then the back substitution.
+static int solve32_enqueue(lu2gpu_ctx *c, int n, const float *a, long ld, int nb, float *v)
+{
+    MixedWork *m = c->mx;
+    for (int i = 0; i < n; i += nb) {
+        const int w = (n - i) < nb ? (n - i) : nb;
+        K_TRY(launch_laswp_scale(v, 1, i, i + w, c->d_ipiv, 0, m->dinv, 0, 1, true, c->stream));
+        K_TRY(launch_trsm_unit_lower_f32(a + (size_t)i * ld + i, ld, v + i, 1, w, 1, nullptr, c->stream));
+        if (i + w < n)
+            K_TRY(launch_gemv_sub(a + (size_t)(i + w) * ld + i, ld, n - i - w, w, v + i, v + i + w, c->stream));
+    }
+    K_TRY(launch_backsolve(a, ld, n, 1, v, 1, c->stream));
+    return 0;
+}
+
+extern "C" int lu2gpu_bf16_update_dev(lu2gpu_ctx *c, int M, int N, int K, const void *a16, long lda, const void *bt16,
+                                      long ldb, float *c32, long ldc, float scale)
+{
+    if (!c || M < 0 || N < 0 || K < 64 || K > 256 || (K % 64) || !a16 || !bt16 || !c32) {
+        set_error("lu2gpu_bf16_update_dev: bad arguments (K must be 64, 128, 192 or 256)");
+        return LU2GPU_ERR_ARG;
+    }
+    DeviceGuard g(c->device);
+    int rc = ensure_work(c, 16, 16, 16);
+    if (rc) return rc;
+    if ((rc = begin_status(c))) return rc;
+    // the scale travels as a device scalar (the factorization computes it on the device)
+    float *dscale = reinterpret_cast<float *>(c->d_bt);
+    CU_TRY(cudaMemcpyAsync(dscale, &scale, sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    K_TRY(launch_bf16_update(a16, lda, bt16, ldb, c32, ldc, M, N, K, dscale, c->d_status, c->stream));
+    return end_status(c, "lu2gpu_bf16_update_dev");
+}
+
+// lumcolumn's panel loop (lu2.c:1126-1141) on the FP32 working matrix
+static int factor32_or_fail(lu2gpu_ctx *c, int n, float *a, long ld, int nb, int mode)
+{
+    View32 v{a, ld, n, n, 0};
+    for (int i = 0; i < n; i += nb) {
+        const int w = (n - i) < nb ? (n - i) : nb;
+        int rc = panel32(c, v, i, w, mode);
+        if (rc) return rc;
+        if ((rc = right_part32(c, v, i, i + w, i + w, n, true))) return rc;
+    }
+    return 0;
+}
+
+extern "C" int lu2gpu_mixed_solve(lu2gpu_ctx *c, int n, const double *a, long lda, const double *b, double *x, int nb,
+                                  int pivot_mode, int max_iter, double *out)
+{
+    if (!c || n <= 0 || !a || !b || !x || lda < n || max_iter < 1) {
+        set_error("lu2gpu_mixed_solve: bad arguments");
+        return LU2GPU_ERR_ARG;
+    }
+    if ((lda & 1) || (reinterpret_cast<uintptr_t>(a) & 15)) {
+        set_error("lu2gpu_mixed_solve: A must be 16-byte aligned with an even row stride");
+        return LU2GPU_ERR_ARG;
+    }
+    if (nb < 64 || nb > 256 || (nb % 64)) {
+        set_error("lu2gpu_mixed_solve: nb=%d must be 64, 128, 192 or 256 (the BF16 update's K)", nb);
+        return LU2GPU_ERR_ARG;
+    }
+    if (pivot_mode != LU2GPU_PIVOT_REF && pivot_mode != LU2GPU_PIVOT_PARTIAL) {
+        set_error("unknown pivot mode %d", pivot_mode);
+        return LU2GPU_ERR_ARG;
+    }
+    DeviceGuard g(c->device);
+    const long ld32 = ((long)n + 31) & ~31L;
+    int rc = mixed_work(c, n, ld32, nb);
+    if (rc) return rc;
+    MixedWork *m = c->mx;
+    double *r = m->vec + n, *rowabs = m->vec + 2 * (size_t)n;
+    float *v32 = reinterpret_cast<float *>(m->vec + 3 * (size_t)n);
+    cudaEvent_t ev[3];
+    for (int i = 0; i < 3; i++) CU_TRY(cudaEventCreate(&ev[i]));
+    if ((rc = begin_status(c))) return rc;
+    CU_TRY(cudaEventRecord(ev[0], c->stream));
+    K_TRY(launch_f64_to_f32(a, lda, m->a32, ld32, n, n, c->stream));
+    if ((rc = factor32_or_fail(c, n, m->a32, ld32, nb, pivot_mode))) return rc;
+    CU_TRY(cudaEventRecord(ev[1], c->stream));
+
+    // refinement: x_0 = 0, r_0 = b; d = LU^{-1} r (FP32), x += d, r = b - A x (FP64)
+    CU_TRY(cudaMemsetAsync(x, 0, (size_t)n * sizeof(double), c->stream));
+    CU_TRY(cudaMemcpyAsync(r, b, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    const double eps = 1.1102230246251565e-16;  // 2^-53
+    double hpl = 0, norms_h[4] = {0, 0, 0, 0};
+    int it = 0;
+    for (it = 1; it <= max_iter; it++) {
+        K_TRY(launch_f64_to_f32(r, 1, v32, 1, n, 1, c->stream));
+        if ((rc = solve32_enqueue(c, n, m->a32, ld32, nb, v32))) return rc;
+        K_TRY(launch_add_f32_to_f64(v32, x, n, c->stream));
+        K_TRY(launch_residual(a, lda, n, b, x, r, it == 1 ? rowabs : nullptr, c->stream));
+        CU_TRY(cudaMemsetAsync(m->norms(), 0, (it == 1 ? 4 : 2) * sizeof(unsigned long long), c->stream));
+        K_TRY(launch_vec_absmax(r, n, m->norms(), c->stream));
+        K_TRY(launch_vec_absmax(x, n, m->norms() + 1, c->stream));
+        if (it == 1) {
+            K_TRY(launch_vec_absmax(b, n, m->norms() + 2, c->stream));
+            K_TRY(launch_vec_absmax(rowabs, n, m->norms() + 3, c->stream));
+        }
+        unsigned long long nb_h[4];
+        CU_TRY(cudaMemcpyAsync(nb_h, m->norms(), (it == 1 ? 4 : 2) * sizeof(unsigned long long),
+                               cudaMemcpyDeviceToHost, c->stream));
+        CU_TRY(cudaStreamSynchronize(c->stream));
+        for (int q = 0; q < (it == 1 ? 4 : 2); q++) memcpy(&norms_h[q], &nb_h[q], sizeof(double));
+        hpl = norms_h[0] / (eps * (norms_h[3] * norms_h[1] + norms_h[2]) * n);
+        if (hpl < 16.0) break;
+    }
+    if (it > max_iter) it = max_iter;
+    CU_TRY(cudaEventRecord(ev[2], c->stream));
+    rc = end_status(c, "lu2gpu_mixed_solve");
+    float t_fac = 0, t_ir = 0;
+    cudaEventElapsedTime(&t_fac, ev[0], ev[1]);
+    cudaEventElapsedTime(&t_ir, ev[1], ev[2]);
+    for (int i = 0; i < 3; i++) cudaEventDestroy(ev[i]);
+    if (out) {
+        out[0] = it;
+        out[1] = hpl;
+        out[2] = t_fac * 1e-3;
+        out[3] = t_ir * 1e-3;
+    }
+    if (rc) return rc;
+    if (hpl >= 16.0) {
+        set_error("lu2gpu_mixed_solve: refinement did not reach a scaled residual < 16 in %d iterations (%.3g)",
+                  max_iter, hpl);
+        return LU2GPU_ERR_NOCONV;
+    }
+    return 0;
 }

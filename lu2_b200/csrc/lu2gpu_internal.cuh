@@ -90,12 +90,16 @@ struct LeafBuffers {
 // by view column; ipiv receives global row numbers (view row + goff).
 cudaError_t launch_leaf(double *a, long ld, int n, int c0, int w, int mode, int goff, int *ipiv, double *dinv,
                         const LeafBuffers &buf, int *status, int max_ctas, cudaStream_t st);
+cudaError_t launch_leaf(float *a, long ld, int n, int c0, int w, int mode, int goff, int *ipiv, float *dinv,
+                        const LeafBuffers &buf, int *status, int max_ctas, cudaStream_t st);
 int leaf_max_ctas(int device);
 
 // Apply the pivots k0..k1-1 (row k <-> row ipiv[k], in order) to columns
 // cs..ce-1 and, when `scale`, multiply row k by dinv[k] after its swap.
 // ipiv holds global rows; the view's row is ipiv[k] - goff.
 cudaError_t launch_laswp_scale(double *a, long ld, int k0, int k1, const int *ipiv, int goff, const double *dinv,
+                               int cs, int ce, bool scale, cudaStream_t st);
+cudaError_t launch_laswp_scale(float *a, long ld, int k0, int k1, const int *ipiv, int goff, const float *dinv,
                                int cs, int ce, bool scale, cudaStream_t st);
 
 // In place X := T^{-1} X for the unit lower triangle T = strict lower part of
@@ -106,6 +110,12 @@ cudaError_t launch_trsm_unit_lower(double *a, long ld, int r0, int K, int cs, in
 // (row stride ldx) given separately; bt may be null.
 cudaError_t launch_trsm_unit_lower_tx(const double *t, long ldt, double *x, long ldx, int K, int ncols, double *bt,
                                       cudaStream_t st);
+// FP32 versions for the precision form; the _bf16 one writes the transposed
+// block row as BF16 multiplied by *bt_scale (a device scalar).
+cudaError_t launch_trsm_unit_lower_f32(const float *t, long ldt, float *x, long ldx, int K, int ncols, float *bt,
+                                       cudaStream_t st);
+cudaError_t launch_trsm_unit_lower_f32_bf16(const float *t, long ldt, float *x, long ldx, int K, int ncols, void *bt,
+                                            const float *bt_scale, cudaStream_t st);
 
 // C[m][n] -= sum_k A[m][k] * Bt[n][k], the trailing update.  A is the
 // row-major matrix starting at (a_row0, a_col0) of `a` (stride ld, rows < a_rows
@@ -125,9 +135,47 @@ cudaError_t launch_transpose(const double *in, long ldi, double *out, long ldo, 
 // lu2.c:110-116); y (n x nrhs, row stride ldx) is overwritten by x.  For lu2's
 // own layout x = a + n, ldx = ld.
 cudaError_t launch_backsolve(const double *a, long ld, int n, int nrhs, double *x, long ldx, cudaStream_t st);
+cudaError_t launch_backsolve(const float *a, long ld, int n, int nrhs, float *x, long ldx, cudaStream_t st);
 
 // out[k] = 1 / a[k][k] (1 for an exactly zero pivot)
 cudaError_t launch_diag_inv(const double *a, long ld, int n, double *out, cudaStream_t st);
+cudaError_t launch_diag_inv(const float *a, long ld, int n, float *out, cudaStream_t st);
+
+// ---------------------------------------------------------------------------
+// precision form (kernels_bf16.cu, kernels_mixed.cu)
+
+// C (FP32, M x N, row-major) -= *scale * A Bt^T with A (M x K) and Bt (N x K)
+// BF16, K-contiguous, K a multiple of 64 and <= 256; tcgen05 (kind::f16).
+cudaError_t launch_bf16_update(const void *a_bf16, long lda, const void *bt_bf16, long ldb, float *c, long ldc, int M,
+                               int N, int K, const float *scale, int *status, cudaStream_t st);
+// out = BF16(in * *scale) for a rows x cols FP32 block
+cudaError_t launch_f32_to_bf16(const float *in, long ldi, void *out, long ldo, int rows, int cols,
+                               const float *scale, cudaStream_t st);
+// C (FP32) -= A Bt^T, A (M x K, stride lda), Bt (N x K, stride K): the
+// updates inside the FP32 panel recursion (CUDA cores, exact FP32)
+cudaError_t launch_sgemm_update(const float *a, long lda, const float *bt, float *c, long ldc, int M, int N, int K,
+                                cudaStream_t st);
+// per-panel power-of-two scales for the BF16 operands: scales[0] = 1/sL,
+// scales[1] = 1/sU, scales[2] = sL*sU with sX = 2^ceil(log2(max|X|)) of the
+// rows x cols block X (called once per block; amax[] accumulates maxima)
+cudaError_t launch_absmax(const float *x, long ld, int rows, int cols, unsigned *amax_bits, cudaStream_t st);
+cudaError_t launch_panel_scales(const unsigned *amax_bits, float *scales, cudaStream_t st);
+// y = FP32(x) for an n x cols FP64 block and back
+cudaError_t launch_f64_to_f32(const double *x, long ldx, float *y, long ldy, int rows, int cols, cudaStream_t st);
+cudaError_t launch_f32_to_f64(const float *x, long ldx, double *y, long ldy, int rows, int cols, cudaStream_t st);
+// r = b - A x (FP64, A n x n stride lda, b and x n-vectors); rowsum (optional)
+// receives sum_j |a_ij| for the HPL norm
+cudaError_t launch_residual(const double *a, long lda, int n, const double *b, const double *x, double *r,
+                            double *rowabs, cudaStream_t st);
+// per-panel update of the forward solve: y[rows] -= L (rows x K, stride ld) * v (K)
+cudaError_t launch_gemv_sub(const float *l, long ld, int rows, int K, const float *v, float *y, cudaStream_t st);
+// bt (N x K BF16) = transpose of u (K x N FP32, stride ld) * *scale
+cudaError_t launch_f32_transpose_bf16(const float *u, long ld, int K, int N, void *bt, const float *scale,
+                                      cudaStream_t st);
+// x += (double) d
+cudaError_t launch_add_f32_to_f64(const float *d, double *x, int n, cudaStream_t st);
+// *out = max(*out, max |v|) as double bits
+cudaError_t launch_vec_absmax(const double *v, int n, unsigned long long *out, cudaStream_t st);
 
 // lu2's matrix generator (randomsetmat, lu2.c:70-85) on the device, bit-identical to
 // glibc drand48: row i holds draws i*(n+1) .. i*(n+1)+n (b_i last); extra

@@ -162,6 +162,21 @@ class Context:
         """Re-solve from stored factors (device a, ipiv) into b (overwritten by x)."""
         _check("lu2gpu_solve", lib().lu2gpu_solve(self._h, n, _ptr(a), lda, nb, _ptr(ipiv), _ptr(b), ldb, nrhs))
 
+    def mixed_solve(self, a, n: int, lda: int, b, x, nb: int = 256, pivot_mode: int = PIVOT_PARTIAL,
+                    max_iter: int = 30) -> dict:
+        """Precision form: FP32/BF16 LU + FP64 iterative refinement (device a, b, x)."""
+        out = np.zeros(4, dtype=np.float64)
+        rc = lib().lu2gpu_mixed_solve(self._h, n, _ptr(a), lda, _ptr(b), _ptr(x), nb, pivot_mode, max_iter, _ptr(out))
+        res = {"status": rc, "iterations": int(out[0]), "hpl": float(out[1]), "factor_s": float(out[2]),
+               "refine_s": float(out[3])}
+        if rc < 0 and rc != -6:
+            raise Lu2GpuError("lu2gpu_mixed_solve", rc)
+        return res
+
+    def bf16_update(self, M, N, K, a16, lda, bt16, ldb, c32, ldc, scale=1.0) -> None:
+        _check("lu2gpu_bf16_update_dev", lib().lu2gpu_bf16_update_dev(self._h, M, N, K, _ptr(a16), lda, _ptr(bt16),
+                                                                       ldb, _ptr(c32), ldc, scale))
+
     def dgemm(self, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc) -> None:
         _check("lu2gpu_dgemm_dev",
                lib().lu2gpu_dgemm_dev(self._h, m, n, k, alpha, _ptr(a), lda, _ptr(b), ldb, beta, _ptr(c), ldc))
