@@ -179,6 +179,70 @@ def read_profile_traffic():
     return None
 
 
+def run_mixed(ctx, n, nb_fp64, ld, buf, dev, stream, args, barrier, max_over_ranks, t_fp64_step, world) -> dict:
+    """BF16-LU + FP64 IR (lu2gpu_mixed_solve) on the diagonally dominant system
+    of order n (lu2's stream with a_ii = sum_j |a_ij|), timed with CUDA events
+    after args.warmup untimed solves; x compared with the plain FP64 GPU LU of
+    the same system.  `buf` (n x ld FP64) is overwritten."""
+    import numpy as np
+    import torch
+
+    import lu2_b200 as L
+
+    nb = args.mixed_nb
+    ctx.generate(buf, n, ld, 1, 1, kind=1)
+    b = buf[:, n].clone()
+    # FP64 reference solution of the same system (untimed)
+    A = buf.clone()
+    if ctx.lusolve(A, n, ld, nb_fp64, 1, L.PIVOT_PARTIAL) != 0:
+        raise RuntimeError("FP64 reference solve hit a zero pivot")
+    x64 = A[:, n].clone()
+    del A
+    torch.cuda.empty_cache()
+    x = torch.zeros(n, dtype=torch.float64, device=dev)
+    res = None
+    for _ in range(args.warmup):
+        res = ctx.mixed_solve(buf, n, ld, b, x, nb)
+    barrier()
+    torch.cuda.synchronize()
+    ts, results = [], []
+    for _ in range(args.steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        res = ctx.mixed_solve(buf, n, ld, b, x, nb)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1) / 1e3)
+        results.append(res)
+    t = max_over_ranks(sum(ts) / len(ts))
+    err = ((x - x64).abs().max() / x64.abs().max()).item()
+    # per-phase split of one more (untimed) solve
+    ctx.set_timing(True)
+    ctx.mixed_solve(buf, n, ld, b, x, nb)
+    timers = ctx.timers()
+    ctx.set_timing(False)
+    upd_ms = timers["DGEMMrest"][0]
+    # algorithmic HBM bytes of the BF16 trailing updates: FP32 C read + written
+    # (8 B) per element per panel plus the BF16 operands (2 B each per element)
+    upd_bytes = 0.0
+    for i in range(0, n, nb):
+        w = min(nb, n - i)
+        m_rows, n_cols = n - i - w, n - i - w
+        upd_bytes += 8.0 * m_rows * n_cols + 2.0 * w * (m_rows + n_cols)
+    value = world * lu_flops(n) / t / 1e9
+    return {"metric": "FP64-equivalent GFLOP/s (2/3 N^3 + 2 N^2)/t", "value": value, "seconds": t,
+            "speedup_vs_fp64_plain": t_fp64_step / t, "n": n, "nb": nb,
+            "matrix": "lu2 drand48 stream, seed 1, diagonal a_ii = sum_j |a_ij| (diagonally dominant)",
+            "iterations": results[-1]["iterations"], "hpl_residual": results[-1]["hpl"],
+            "factor_s": results[-1]["factor_s"], "refine_s": results[-1]["refine_s"],
+            "x_rel_err_vs_fp64_lu": err, "steps": len(ts), "warmup": args.warmup,
+            "bf16_update": {"ms": upd_ms, "launches": timers["DGEMMrest"][1],
+                            "hbm_gbs": upd_bytes / (upd_ms / 1e3) / 1e9 if upd_ms > 0 else None,
+                            "algorithmic_bytes": upd_bytes},
+            "phases_ms": {k: {"ms": v[0], "launches": v[1]} for k, v in timers.items()}}
+
+
 def run_reference(args, rank: int) -> None:
     if rank != 0:
         return
@@ -222,8 +286,12 @@ def main() -> int:
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the BF16-LU + IR measurement")
+    ap.add_argument("--mixed-nb", type=int, default=256)
     ap.add_argument("--profile", action="store_true",
                     help="profiling run for ncu: generate the matrix and run exactly one factor+solve step")
+    ap.add_argument("--profile-mixed", action="store_true",
+                    help="profiling run for ncu: one BF16-LU + IR solve of the diagonally dominant system")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -275,6 +343,15 @@ def main() -> int:
         if info != 0:
             raise RuntimeError("zero pivot at column %d" % (info - 1))
 
+    if args.profile_mixed:
+        ctx.generate(pristine, n, ld, 1, 1, kind=1)
+        b = pristine[:, n].clone()
+        x = torch.zeros(n, dtype=torch.float64, device=dev)
+        res = ctx.mixed_solve(pristine, n, ld, b, x, args.mixed_nb)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_mixed": res, "n": n}))
+        ctx.close()
+        return 0
     if args.profile:
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -366,6 +443,16 @@ def main() -> int:
         lib.lu2gpu_release()
         del host, bvec
 
+    # precision form (configs C3): BF16-LU + FP64 iterative refinement on the
+    # diagonally dominant system of the same order, against this run's FP64 LU
+    forms = {}
+    if not args.no_mixed:
+        if "A" in locals():
+            del A
+        torch.cuda.empty_cache()
+        forms["bf16_ir"] = run_mixed(ctx, n, nb, ld, pristine, dev, stream, args, barrier, max_over_ranks,
+                                     t / args.steps, world)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_reference_gflops(REF_SAMPLE_N, nb, 2)
@@ -380,7 +467,7 @@ def main() -> int:
                           "parallelism": "replicas" if world > 1 else "single",
                           "l2": "inputs (%.1f GB) larger than L2, no flush" % (n * ld * 8 / 1e9)},
                "gpu_launches": int(launches), "hpl_residual": hplres, "clocks": clk, "roofline": roofline,
-               "phases_ms": phases, "e2e": e2e, "cpu_baseline": cpu}
+               "phases_ms": phases, "e2e": e2e, "cpu_baseline": cpu, "forms": forms}
         print(json.dumps(out))
     ctx.close()
     if world > 1:

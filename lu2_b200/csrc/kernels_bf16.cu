@@ -2,12 +2,15 @@
 // generation tensor cores: C (FP32, row-major) -= scale * A * Bt^T with A
 // (M x K) and Bt (N x K) in BF16, both K-contiguous.
 //
-// Per CTA one 128 x BN tile: TMA brings all K (<= 256) of both operands into
-// shared memory (128-byte swizzled boxes of 64 BF16 along K, one mbarrier per
-// 64-wide k block), one thread issues tcgen05.mma (kind::f16, BF16 inputs,
-// FP32 accumulator in tensor memory, 128 x BN x 16 per instruction) as each k
-// block lands, commits to an mbarrier, and the four warps read their 32 TMEM
-// lanes (= tile rows) back with tcgen05.ld and update C in global memory.
+// Per CTA one 128 x BN tile: TMA streams both operands through two shared
+// memory stages (128-byte swizzled boxes of 64 BF16 along K, full/empty
+// mbarriers per stage), one thread issues tcgen05.mma (kind::f16, BF16
+// inputs, FP32 accumulator in tensor memory, 128 x BN x 16 per instruction)
+// as each k block lands and releases the stage with tcgen05.commit.  Every
+// thread loads its tile row of C (TMEM lane = row) into registers while that
+// runs, then reads the accumulator with tcgen05.ld and writes C - scale*acc.
+// The small footprint (65 KB of shared memory, 128 TMEM columns) lets two
+// CTAs share an SM, so one CTA's C traffic overlaps the other's MMAs.
 //
 // The update this replaces is lu2's mmmulandsub -> mydgemm (lu2.c:312-343,
 // lu2lib.c:2079); the precision form keeps lu2's algorithm and storage, in
@@ -76,13 +79,16 @@ struct Bf16Params {
     int *status;
 };
 
+constexpr int UB_STAGES = 2;  // 64-wide k blocks in flight per CTA
+
 template <int BN>
-__global__ void __launch_bounds__(UB_THREADS, 1)
+__global__ void __launch_bounds__(UB_THREADS, 2)
     bf16_update_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, Bf16Params p)
 {
     constexpr int A_BYTES = UB_BM * 128, B_BYTES = BN * 128, STAGE = A_BYTES + B_BYTES;
     extern __shared__ uint8_t smem_raw[];
-    __shared__ __align__(8) uint64_t full_bar[UB_KMAX / UB_BK];
+    __shared__ __align__(8) uint64_t full_bar[UB_STAGES];
+    __shared__ __align__(8) uint64_t empty_bar[UB_STAGES];
     __shared__ __align__(8) uint64_t mma_bar;
     __shared__ uint32_t s_tmem;
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -103,8 +109,10 @@ __global__ void __launch_bounds__(UB_THREADS, 1)
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
-        for (int s = 0; s < KB; s++)
+        for (int s = 0; s < UB_STAGES; s++) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&full_bar[s])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&empty_bar[s])) : "memory");
+        }
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&mma_bar)) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -113,32 +121,65 @@ __global__ void __launch_bounds__(UB_THREADS, 1)
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = s_tmem;
 
-    bool ok = true;
-    if (tid == 0) {
-        for (int kb = 0; kb < KB; kb++) {
-            uint8_t *sa = smem + kb * STAGE;
-            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&full_bar[kb])),
-                         "r"(STAGE)
-                         : "memory");
-            asm volatile(
-                "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
-                "[%4];" ::"r"(smem_addr(sa)),
-                "l"(&tmA), "r"(kb * UB_BK), "r"(m0), "r"(smem_addr(&full_bar[kb]))
-                : "memory");
-            asm volatile(
-                "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
-                "[%4];" ::"r"(smem_addr(sa + A_BYTES)),
-                "l"(&tmB), "r"(kb * UB_BK), "r"(n0), "r"(smem_addr(&full_bar[kb]))
-                : "memory");
+    auto issue = [&](int kb, int s) {
+        uint8_t *sa = smem + s * STAGE;
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&full_bar[s])),
+                     "r"(STAGE)
+                     : "memory");
+        asm volatile(
+            "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+            "[%4];" ::"r"(smem_addr(sa)),
+            "l"(&tmA), "r"(kb * UB_BK), "r"(m0), "r"(smem_addr(&full_bar[s]))
+            : "memory");
+        asm volatile(
+            "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+            "[%4];" ::"r"(smem_addr(sa + A_BYTES)),
+            "l"(&tmB), "r"(kb * UB_BK), "r"(n0), "r"(smem_addr(&full_bar[s]))
+            : "memory");
+    };
+    if (tid == 0)
+        for (int kb = 0; kb < UB_STAGES && kb < KB; kb++) issue(kb, kb);
+
+    // each thread's tile row of C (TMEM lane = row), loaded while the operands
+    // stream in and the MMAs run
+    const int row = warp * 32 + lane;
+    const int m = m0 + row;
+    const bool rowok = m < p.M;
+    float *crow = p.C + (size_t)(rowok ? m : 0) * p.ldc + n0;
+    const bool vec = rowok && n0 + BN <= p.N && ((reinterpret_cast<uintptr_t>(crow) & 15) == 0);
+    float4 cv[BN / 4];
+#pragma unroll
+    for (int q = 0; q < BN / 4; q++) {
+        if (vec) {
+            cv[q] = *reinterpret_cast<const float4 *>(crow + 4 * q);
+        } else {
+            float e[4] = {0.f, 0.f, 0.f, 0.f};
+            for (int j = 0; j < 4; j++)
+                if (rowok && n0 + 4 * q + j < p.N) e[j] = crow[4 * q + j];
+            cv[q] = make_float4(e[0], e[1], e[2], e[3]);
         }
+    }
+
+    if (tid == 0) {
         constexpr uint32_t idesc = umma_idesc_bf16(UB_BM, BN);
+        bool ok = true;
         for (int kb = 0; kb < KB && ok; kb++) {
-            if (!mbar_wait_limit(&full_bar[kb], 0, p.status, 5)) {
+            // refill the stage the previous k block used, once its MMAs are done
+            if (kb >= 1 && kb - 1 + UB_STAGES < KB) {
+                const int ps = (kb - 1) % UB_STAGES;
+                if (!mbar_wait_limit(&empty_bar[ps], (uint32_t)((kb - 1) / UB_STAGES) & 1u, p.status, 7)) {
+                    ok = false;
+                    break;
+                }
+                issue(kb - 1 + UB_STAGES, ps);
+            }
+            const int s = kb % UB_STAGES;
+            if (!mbar_wait_limit(&full_bar[s], (uint32_t)(kb / UB_STAGES) & 1u, p.status, 5)) {
                 ok = false;
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t sa = smem_addr(smem + kb * STAGE), sb = sa + A_BYTES;
+            const uint32_t sa = smem_addr(smem + s * STAGE), sb = sa + A_BYTES;
 #pragma unroll
             for (int kk = 0; kk < UB_BK / 16; kk++) {
                 const uint64_t da = umma_desc_sw128(sa + kk * 32), db = umma_desc_sw128(sb + kk * 32);
@@ -150,9 +191,11 @@ __global__ void __launch_bounds__(UB_THREADS, 1)
                     "l"(da), "l"(db), "r"(idesc), "r"(acc)
                     : "memory");
             }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_addr(&empty_bar[s]))
+                         : "memory");
         }
-        // arrives once every MMA issued above has completed (also on failure, so
-        // the epilogue's wait ends and no TMA is left in flight unobserved)
+        // arrives once every MMA issued above has completed
         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                          smem_addr(&mma_bar))
                      : "memory");
@@ -160,14 +203,11 @@ __global__ void __launch_bounds__(UB_THREADS, 1)
     __syncwarp();
     const bool done = mbar_wait_limit(&mma_bar, 0, p.status, 6);
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const int *st = p.status;
-    const bool good = done && *(volatile const int *)&st[1] == 0;
-
-    // epilogue: warp w owns TMEM lanes 32w..32w+31 = tile rows; 32 columns per load
-    const int row = warp * 32 + lane;
-    const int m = m0 + row;
+    const bool good = done && *(volatile const int *)&p.status[1] == 0;
     const float scale = *p.scale;
-#pragma unroll 1
+
+    // epilogue: warp w owns TMEM lanes 32w..32w+31 (its tile rows); 32 columns per load
+#pragma unroll
     for (int cb = 0; cb < BN / 32; cb++) {
         uint32_t r[32];
         const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(cb * 32);
@@ -181,23 +221,25 @@ __global__ void __launch_bounds__(UB_THREADS, 1)
               "=r"(r[30]), "=r"(r[31])
             : "r"(taddr));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (!good || m >= p.M) continue;
-        const int nb0 = n0 + cb * 32;
-        float *crow = p.C + (size_t)m * p.ldc + nb0;
-        if (nb0 + 32 <= p.N && ((reinterpret_cast<uintptr_t>(crow) & 15) == 0)) {
 #pragma unroll
-            for (int j = 0; j < 32; j += 4) {
-                float4 c = *reinterpret_cast<float4 *>(crow + j);
-                c.x -= scale * __uint_as_float(r[j]);
-                c.y -= scale * __uint_as_float(r[j + 1]);
-                c.z -= scale * __uint_as_float(r[j + 2]);
-                c.w -= scale * __uint_as_float(r[j + 3]);
-                *reinterpret_cast<float4 *>(crow + j) = c;
+        for (int q = 0; q < 8; q++) {
+            float4 &c = cv[cb * 8 + q];
+            c.x -= scale * __uint_as_float(r[4 * q]);
+            c.y -= scale * __uint_as_float(r[4 * q + 1]);
+            c.z -= scale * __uint_as_float(r[4 * q + 2]);
+            c.w -= scale * __uint_as_float(r[4 * q + 3]);
+        }
+    }
+    if (good && rowok) {
+#pragma unroll
+        for (int q = 0; q < BN / 4; q++) {
+            if (vec) {
+                *reinterpret_cast<float4 *>(crow + 4 * q) = cv[q];
+            } else {
+                const float e[4] = {cv[q].x, cv[q].y, cv[q].z, cv[q].w};
+                for (int j = 0; j < 4; j++)
+                    if (n0 + 4 * q + j < p.N) crow[4 * q + j] = e[j];
             }
-        } else {
-#pragma unroll
-            for (int j = 0; j < 32; j++)
-                if (nb0 + j < p.N) crow[j] -= scale * __uint_as_float(r[j]);
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -258,7 +300,7 @@ cudaError_t launch_bf16_update(const void *a_bf16, long lda, const void *bt_bf16
     p.tiles_n = (N + BN - 1) / BN;
     p.group_m = 16;
     p.status = status;
-    const int smem = (K / UB_BK) * (UB_BM * 128 + BN * 128) + 1024;
+    const int smem = UB_STAGES * (UB_BM * 128 + BN * 128) + 1024;
     e = cudaFuncSetAttribute(bf16_update_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     const long tiles = (long)p.tiles_m * p.tiles_n;
