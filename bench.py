@@ -243,6 +243,63 @@ def run_mixed(ctx, n, nb_fp64, ld, buf, dev, stream, args, barrier, max_over_ran
             "phases_ms": {k: {"ms": v[0], "launches": v[1]} for k, v in timers.items()}}
 
 
+def run_batched(ctx, dev, stream, args, max_over_ranks, world) -> dict:
+    """Batching form: 20,000 systems, N log-uniform in [16, 512]
+    (seed 1), 10% with 8 right-hand sides, each lu2's stream with seed 1+i; FP64,
+    one persistent launch replayed from a CUDA graph, launch shape autotuned.
+    Compared with a loop of single plain-method solves (lu2gpu_lusolve, nb=64)
+    over a sample of the same systems."""
+    import numpy as np
+    import torch
+
+    import lu2_b200 as L
+
+    count = args.batch_count
+    n, r = L.batch_sizes(count, 1, 16, 512, 0.1, 8)
+    b = L.Batch(ctx, n, r)
+    b.generate(1)
+    b.snapshot()
+    cfg = b.autotune()
+    for _ in range(args.warmup):
+        b.restore()
+        b.solve()
+    ts = []
+    for _ in range(args.steps):
+        b.restore()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        info = b.solve()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1) / 1e3)
+    t = max_over_ranks(sum(ts) / len(ts))
+    res = b.residuals()
+    flops = float(np.sum(2.0 / 3.0 * n.astype(np.float64) ** 3 + 2.0 * n.astype(np.float64) ** 2 * r))
+    # the loop of single plain-method launches, on a sample of systems
+    rng = np.random.default_rng(0)
+    sample = rng.choice(count, size=min(args.batch_loop_sample, count), replace=False)
+    b.restore()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in sample:
+        ptr, ld = b.system(int(i))
+        ctx.lusolve(ptr, int(n[i]), ld, 64, int(r[i]), L.PIVOT_PARTIAL)
+    torch.cuda.synchronize()
+    t_loop = (time.perf_counter() - t0) / len(sample)
+    b.close()
+    sps = world * count / t
+    return {"metric": "batched solves/s", "value": sps, "unit": "systems/s", "seconds": t, "systems": count,
+            "gflops": world * flops / t / 1e9, "flops": flops,
+            "sizes": "N log-uniform in [16, 512] (seed 1), 10% with 8 right-hand sides, entries lu2 stream seed 1+i",
+            "max_hpl_residual": float(res.max()), "all_below_16": bool((res < 16).all()),
+            "zero_pivots": int((info != 0).sum()), "autotuned": cfg, "steps": len(ts), "warmup": args.warmup,
+            "loop_baseline": {"solves_per_s": 1.0 / t_loop, "sample_systems": int(len(sample)),
+                              "api": "lu2gpu_lusolve per system (nb=64), host-timed loop"},
+            "speedup_vs_loop": sps / (world / t_loop)}
+
+
 def run_reference(args, rank: int) -> None:
     if rank != 0:
         return
@@ -288,6 +345,9 @@ def main() -> int:
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the BF16-LU + IR measurement")
     ap.add_argument("--mixed-nb", type=int, default=256)
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-systems measurement")
+    ap.add_argument("--batch-count", type=int, default=20000)
+    ap.add_argument("--batch-loop-sample", type=int, default=400)
     ap.add_argument("--profile", action="store_true",
                     help="profiling run for ncu: generate the matrix and run exactly one factor+solve step")
     ap.add_argument("--profile-mixed", action="store_true",
@@ -443,7 +503,7 @@ def main() -> int:
         lib.lu2gpu_release()
         del host, bvec
 
-    # precision form (configs C3): BF16-LU + FP64 iterative refinement on the
+    # precision form: BF16-LU + FP64 iterative refinement on the
     # diagonally dominant system of the same order, against this run's FP64 LU
     forms = {}
     if not args.no_mixed:
@@ -452,6 +512,10 @@ def main() -> int:
         torch.cuda.empty_cache()
         forms["bf16_ir"] = run_mixed(ctx, n, nb, ld, pristine, dev, stream, args, barrier, max_over_ranks,
                                      t / args.steps, world)
+    if not args.no_batched:
+        del pristine
+        torch.cuda.empty_cache()
+        forms["batched_fp64"] = run_batched(ctx, dev, stream, args, max_over_ranks, world)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

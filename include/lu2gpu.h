@@ -69,6 +69,29 @@ extern "C" {
  * or the environment variable LU2GPU_PIVOT=ref selects the reference's. */
 void lumcolumn(int n, double *a, double *b, int m, double *awork, int *pv, int recursive);
 
+/* lu2.c's per-panel steps on the host matrix a[n][n+16] (each stages the
+ * region it touches through the GPU; pivot mode as for lumcolumn):
+ *  column_decomposition_recursive (lu2.c:1088-1120): factor the panel of
+ *    columns i..i+m-1, rows i..n-1; pv[0..m) receives the pivot rows.
+ *  process_right_part (lu2.c:524-581): apply pv[0..m) with the 1/pivot row
+ *    scaling to columns i+m..iend-1, solve the U block row, update rows
+ *    i+m..n-1 (m a multiple of 16 or not).
+ *  backward_sub (lu2.c:110-116): b = x from the unit upper factor and column n.
+ * awork is accepted and unused. */
+void column_decomposition_recursive(int n, double *a, int m, double *awork, int *pv, int i);
+void process_right_part(int n, double *a, int m, double *awork, int *pv, int i, int iend);
+void backward_sub(int n, double *a, double *b);
+
+/* lu2tlib.h:1-18, the column-major slab API (a[j][r] at a + j*n + r, i.e.
+ * double a[n+1][n]): cm_column_decomposition_recursive (lu2tlib.c:1095-1128)
+ * and cm_column_decomposition (lu2tlib.c:1041-1066, at most 16 columns; in
+ * reference pivot mode every column searches the slab's first column, as
+ * there) factor slab columns 0..m-1, rows i..n-1; cm_process_right_part
+ * (lu2tlib.c:1068-1093) updates slab columns m..iend-i-1. */
+void cm_column_decomposition_recursive(int n, double *a, int m, int *pv, int i);
+void cm_column_decomposition(int n, double *a, int m, int *pv, int i);
+void cm_process_right_part(int n, double *a, int m, int *pv, int i, int iend);
+
 /* lu2lib.h:9-19, lu2lib.c:2079-2136: row-major C = alpha*A*B + beta*C. */
 void mydgemm(int m, int n, int k, double alpha, double *a, int na, double *b, int nb, double beta, double *c,
              int nc);
@@ -179,6 +202,37 @@ int lu2gpu_mixed_solve(lu2gpu_ctx *ctx, int n, const double *a, long lda, const 
  * 192, 256}; tcgen05 tensor cores with FP32 accumulation. */
 int lu2gpu_bf16_update_dev(lu2gpu_ctx *ctx, int M, int N, int K, const void *a, long lda, const void *bt, long ldb,
                            float *c, long ldc, float scale);
+
+/* Batching form (no counterpart in the reference, which solves one system
+ * per run): many independent systems of uneven order, each lu2's augmented
+ * problem (row-major, b in columns n..n+nrhs-1, x replaces b) solved with
+ * lu2's algorithm, all in one persistent launch replayed from a CUDA graph. */
+typedef struct lu2gpu_batch lu2gpu_batch;
+/* Describe count systems (orders n[i] <= 4096, nrhs[i] <= 64 right-hand
+ * sides; nrhs may be NULL for one each) and allocate their packed storage. */
+int lu2gpu_batch_create(lu2gpu_ctx *ctx, int count, const int *n, const int *nrhs, lu2gpu_batch **out);
+int lu2gpu_batch_destroy(lu2gpu_batch *b);
+/* Device pointer to system i's augmented matrix and its row stride. */
+int lu2gpu_batch_system(lu2gpu_batch *b, int i, double **a, long *ld);
+/* System i := lu2's randomsetmat stream with seed (seed + i). */
+int lu2gpu_batch_generate(lu2gpu_batch *b, long seed);
+/* Keep a copy of the current systems (for residuals and for re-running). */
+int lu2gpu_batch_snapshot(lu2gpu_batch *b);
+int lu2gpu_batch_restore(lu2gpu_batch *b);
+/* Launch shape: threads per CTA, panel width of the blocked path, CTAs per SM. */
+int lu2gpu_batch_set_config(lu2gpu_batch *b, int threads, int pw, int ctas_per_sm);
+/* Time the launch shapes on this batch and keep the fastest; params_out (4
+ * ints, may be NULL) = {threads, panel width, CTAs per SM, microseconds}. */
+int lu2gpu_batch_autotune(lu2gpu_batch *b, int *params_out);
+/* Factor and solve all systems in place; info_host (count ints, may be NULL)
+ * receives each system's zero-pivot status (0 or column + 1). */
+int lu2gpu_batch_solve(lu2gpu_batch *b, int *info_host);
+/* HPL scaled residual of every system against the snapshot (host out[count]). */
+int lu2gpu_batch_residuals(lu2gpu_batch *b, double *out_host);
+/* Orders log-uniform in [nmin, nmax] and, for a fraction frac_multi of the
+ * systems, nrhs_multi right-hand sides, from a seeded drand48 stream. */
+int lu2gpu_batch_sizes(int count, long seed, int nmin, int nmax, double frac_multi, int nrhs_multi, int *n_out,
+                       int *nrhs_out);
 
 /* Row-major device DGEMM, C = alpha*A*B + beta*C (mydgemm's contract). */
 int lu2gpu_dgemm_dev(lu2gpu_ctx *ctx, int m, int n, int k, double alpha, const double *a, long lda, const double *b,

@@ -8,8 +8,10 @@ from .lu2 import (  # noqa: F401
     CBLAS_TRANS,
     PIVOT_PARTIAL,
     PIVOT_REF,
+    Batch,
     Context,
     Lu2GpuError,
+    batch_sizes,
     device_ld,
     gdr_dgemm_,
     gdrblas_dgemm,

@@ -21,6 +21,12 @@ vp = C.c_void_p
 # argtypes of every exported function (names as in include/lu2gpu.h)
 SIGNATURES = {
     "lumcolumn": (None, [C.c_int, vp, vp, C.c_int, vp, vp, C.c_int]),
+    "column_decomposition_recursive": (None, [C.c_int, vp, C.c_int, vp, vp, C.c_int]),
+    "process_right_part": (None, [C.c_int, vp, C.c_int, vp, vp, C.c_int, C.c_int]),
+    "backward_sub": (None, [C.c_int, vp, vp]),
+    "cm_column_decomposition_recursive": (None, [C.c_int, vp, C.c_int, vp, C.c_int]),
+    "cm_column_decomposition": (None, [C.c_int, vp, C.c_int, vp, C.c_int]),
+    "cm_process_right_part": (None, [C.c_int, vp, C.c_int, vp, C.c_int, C.c_int]),
     "mydgemm": (None, [C.c_int, C.c_int, C.c_int, C.c_double, vp, C.c_int, vp, C.c_int, C.c_double, vp, C.c_int]),
     "matmul_for_small_nk": (None, [C.c_int, vp, C.c_int, vp, C.c_int, vp, C.c_int, C.c_int, C.c_int]),
     "reset_gdr": (None, [C.c_int, vp, C.c_int, vp, C.c_int]),
@@ -50,6 +56,17 @@ SIGNATURES = {
     "lu2gpu_mixed_solve": (C.c_int, [vp, C.c_int, vp, C.c_long, vp, vp, C.c_int, C.c_int, C.c_int, vp]),
     "lu2gpu_bf16_update_dev": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, vp, C.c_long, vp, C.c_long, vp, C.c_long,
                                          C.c_float]),
+    "lu2gpu_batch_create": (C.c_int, [vp, C.c_int, vp, vp, C.POINTER(vp)]),
+    "lu2gpu_batch_destroy": (C.c_int, [vp]),
+    "lu2gpu_batch_system": (C.c_int, [vp, C.c_int, C.POINTER(vp), C.POINTER(C.c_long)]),
+    "lu2gpu_batch_generate": (C.c_int, [vp, C.c_long]),
+    "lu2gpu_batch_snapshot": (C.c_int, [vp]),
+    "lu2gpu_batch_restore": (C.c_int, [vp]),
+    "lu2gpu_batch_set_config": (C.c_int, [vp, C.c_int, C.c_int, C.c_int]),
+    "lu2gpu_batch_autotune": (C.c_int, [vp, vp]),
+    "lu2gpu_batch_solve": (C.c_int, [vp, vp]),
+    "lu2gpu_batch_residuals": (C.c_int, [vp, vp]),
+    "lu2gpu_batch_sizes": (C.c_int, [C.c_int, C.c_long, C.c_int, C.c_int, C.c_double, C.c_int, vp, vp]),
     "lu2gpu_generate": (C.c_int, [vp, C.c_int, C.c_int, C.c_long, C.c_int, vp, C.c_long]),
     "lu2gpu_dgemm_dev": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_double, vp, C.c_long, vp, C.c_long,
                                    C.c_double, vp, C.c_long]),

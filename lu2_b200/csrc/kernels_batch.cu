@@ -1,0 +1,447 @@
+// kernels_batch.cu -- the batching form: thousands of independent dense
+// systems of uneven order factored and solved by one persistent launch.
+//
+// Every system is lu2's augmented problem (row-major, b in the columns
+// n..n+nrhs-1, lu2.c:28) and is solved with lu2's algorithm: partial pivoting
+// with the first maximal |a| (lu2tlib.c:42-52), the pivot row scaled by
+// 1/pivot (lu2tlib.c:1057-1059, lu2.c:551-552), right-looking updates that
+// carry the right-hand sides along (lu2.c:1138), then the unit-upper back
+// substitution (lu2.c:110-116).  x overwrites b.
+//
+// CTAs take systems from a queue ordered largest first (an atomic counter over
+// a host-sorted order).  A system whose augmented matrix fits the shared
+// memory budget is factored and solved there; larger ones run a blocked LU on
+// the L2-resident matrix with the panel (all remaining rows x pw columns) in
+// shared memory and the trailing update computed from a shared-memory copy of
+// the U block in 4 x 4 register tiles.
+#include <climits>
+
+#include "lu2gpu_internal.cuh"
+
+namespace lu2gpu {
+
+__device__ __forceinline__ void batch_block_argmax(double &v, int &i, double *s_v, int *s_i)
+{
+    warp_argmax(v, i);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    if (lane == 0) {
+        s_v[warp] = v;
+        s_i[warp] = i;
+    }
+    __syncthreads();
+    v = lane < nw ? s_v[lane] : -1.0;
+    i = lane < nw ? s_i[lane] : INT_MAX;
+    warp_argmax(v, i);  // every warp reduces the same partials
+    __syncthreads();    // partials read before the next reduction writes them
+}
+
+// whole system in shared memory: S (n x nc, stride nc)
+__device__ void batch_solve_smem(double *A, long ld, int n, int nrhs, double *S, int *info, double *s_v, int *s_i)
+{
+    const int nc = n + nrhs, T = blockDim.x, tid = threadIdx.x;
+    for (int idx = tid; idx < n * nc; idx += T) {
+        const int r = idx / nc, c = idx - r * nc;
+        S[idx] = A[(size_t)r * ld + c];
+    }
+    __syncthreads();
+    int first_zero = 0;
+    for (int k = 0; k < n; k++) {
+        double v = -1.0;
+        int p = INT_MAX;
+        for (int r = k + tid; r < n; r += T) {
+            const double a = fabs(S[r * nc + k]);
+            if (a > v) {
+                v = a;
+                p = r;
+            }
+        }
+        batch_block_argmax(v, p, s_v, s_i);
+        if (p == INT_MAX) p = k;
+        if (p != k)
+            for (int c = tid; c < nc; c += T) {
+                const double t = S[k * nc + c];
+                S[k * nc + c] = S[p * nc + c];
+                S[p * nc + c] = t;
+            }
+        __syncthreads();
+        const double d = S[k * nc + k];
+        if (d == 0.0) {
+            if (!first_zero) first_zero = k + 1;
+            __syncthreads();
+            continue;
+        }
+        const double inv = 1.0 / d;
+        for (int c = k + 1 + tid; c < nc; c += T) S[k * nc + c] *= inv;
+        __syncthreads();
+        const int w = nc - k - 1, h = n - k - 1;
+        for (int idx = tid; idx < h * w; idx += T) {
+            const int r = k + 1 + idx / w, c = k + 1 + idx % w;
+            S[r * nc + c] -= S[r * nc + k] * S[k * nc + c];
+        }
+        __syncthreads();
+    }
+    for (int j = n - 1; j >= 1; j--) {
+        for (int idx = tid; idx < j * nrhs; idx += T) {
+            const int i = idx / nrhs, q = idx - i * nrhs;
+            S[i * nc + n + q] -= S[i * nc + j] * S[j * nc + n + q];
+        }
+        __syncthreads();
+    }
+    for (int idx = tid; idx < n * nrhs; idx += T) {
+        const int r = idx / nrhs, q = idx - r * nrhs;
+        A[(size_t)r * ld + n + q] = S[r * nc + n + q];
+    }
+    if (tid == 0) *info = first_zero;
+}
+
+// blocked LU in global memory (L2-resident), panel of pw columns in shared memory
+__device__ void batch_solve_blocked(double *A, long ld, int n, int nrhs, int pw, double *P, double *U, int *piv,
+                                    double *dinv, int *info, double *s_v, int *s_i)
+{
+    const int nc = n + nrhs, T = blockDim.x, tid = threadIdx.x;
+    int first_zero = 0;
+    for (int k0 = 0; k0 < n; k0 += pw) {
+        const int w = min(pw, n - k0), rows = n - k0;
+        // panel rows k0..n-1, columns k0..k0+w-1 -> P (rows x pw)
+        for (int idx = tid; idx < rows * w; idx += T) {
+            const int r = idx / w, c = idx - r * w;
+            P[r * pw + c] = A[(size_t)(k0 + r) * ld + k0 + c];
+        }
+        __syncthreads();
+        for (int c = 0; c < w; c++) {
+            double v = -1.0;
+            int p = INT_MAX;
+            for (int r = c + tid; r < rows; r += T) {
+                const double a = fabs(P[r * pw + c]);
+                if (a > v) {
+                    v = a;
+                    p = r;
+                }
+            }
+            batch_block_argmax(v, p, s_v, s_i);
+            if (p == INT_MAX) p = c;
+            if (tid == 0) piv[c] = p;
+            if (p != c)
+                for (int j = tid; j < w; j += T) {
+                    const double t = P[c * pw + j];
+                    P[c * pw + j] = P[p * pw + j];
+                    P[p * pw + j] = t;
+                }
+            __syncthreads();
+            const double d = P[c * pw + c];
+            const bool zero = (d == 0.0);
+            if (zero && !first_zero) first_zero = k0 + c + 1;
+            const double inv = zero ? 1.0 : 1.0 / d;
+            if (tid == 0) dinv[c] = inv;
+            if (!zero)
+                for (int j = tid; j < w; j += T)
+                    if (j != c) P[c * pw + j] *= inv;
+            __syncthreads();
+            if (!zero) {
+                const int wj = w - c - 1, hr = rows - c - 1;
+                for (int idx = tid; idx < hr * wj; idx += T) {
+                    const int r = c + 1 + idx / wj, j = c + 1 + idx % wj;
+                    P[r * pw + j] -= P[r * pw + c] * P[c * pw + j];
+                }
+            }
+            __syncthreads();
+        }
+        for (int idx = tid; idx < rows * w; idx += T) {
+            const int r = idx / w, c = idx - r * w;
+            A[(size_t)(k0 + r) * ld + k0 + c] = P[r * pw + c];
+        }
+        __syncthreads();
+        // right part: exchanges with 1/pivot scaling, then the unit-lower solve
+        // of the U block rows, one thread per column (lu2.c:524-581)
+        const int cs = k0 + w;
+        for (int j = cs + tid; j < nc; j += T) {
+            double x[64];
+            for (int c = 0; c < w; c++) {
+                const int p = piv[c];
+                double *rc = A + (size_t)(k0 + c) * ld + j;
+                double vc = *rc;
+                if (p != c) {
+                    double *rp = A + (size_t)(k0 + p) * ld + j;
+                    const double vp = *rp;
+                    *rp = vc;
+                    vc = vp;
+                }
+                x[c] = vc * dinv[c];
+            }
+            for (int r = 1; r < w; r++) {
+                double s = x[r];
+                for (int l = 0; l < r; l++) s -= P[r * pw + l] * x[l];
+                x[r] = s;
+            }
+            for (int c = 0; c < w; c++) A[(size_t)(k0 + c) * ld + j] = x[c];
+        }
+        __syncthreads();
+        // trailing update A[k0+w.., cs..] -= L21 U12 in 64-column chunks
+        const int h = n - cs;
+        for (int c0 = cs; c0 < nc && h > 0; c0 += 64) {
+            const int cw = min(64, nc - c0);
+            for (int idx = tid; idx < w * 64; idx += T) {
+                const int l = idx >> 6, c = idx & 63;
+                U[l * 64 + c] = (c < cw) ? A[(size_t)(k0 + l) * ld + c0 + c] : 0.0;
+            }
+            __syncthreads();
+            const int tx = tid & 15, ty = tid >> 4, tys = T >> 4;
+            for (int rb = ty * 4; rb < h; rb += tys * 4) {
+                double acc[4][4] = {};
+                for (int l = 0; l < w; l++) {
+                    double av[4], bv[4];
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        av[i] = (rb + i < h) ? P[(w + rb + i) * pw + l] : 0.0;
+                        bv[i] = U[l * 64 + tx * 4 + i];
+                    }
+#pragma unroll
+                    for (int i = 0; i < 4; i++)
+#pragma unroll
+                        for (int q = 0; q < 4; q++) acc[i][q] = fma(av[i], bv[q], acc[i][q]);
+                }
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    if (rb + i >= h) break;
+                    double *row = A + (size_t)(cs + rb + i) * ld + c0;
+#pragma unroll
+                    for (int q = 0; q < 4; q++)
+                        if (tx * 4 + q < cw) row[tx * 4 + q] -= acc[i][q];
+                }
+            }
+            __syncthreads();
+        }
+    }
+    // back substitution with the unit upper factor (lu2.c:110-116), blocked by
+    // 32 rows: y (n x nrhs) and each 32 x 32 diagonal block in shared memory
+    // (reusing the panel's space), the rows above updated from their 32-wide
+    // row segments
+    double *Y = P;
+    double *Ud = P + (size_t)n * nrhs;  // 32 x 33
+    for (int idx = tid; idx < n * nrhs; idx += T) {
+        const int r = idx / nrhs, q = idx - r * nrhs;
+        Y[idx] = A[(size_t)r * ld + n + q];
+    }
+    __syncthreads();
+    for (int jb = ((n - 1) / 32) * 32; jb >= 0; jb -= 32) {
+        const int je = min(jb + 32, n), bw = je - jb;
+        for (int idx = tid; idx < bw * bw; idx += T) {
+            const int i = idx / bw, j = idx - i * bw;
+            Ud[i * 33 + j] = A[(size_t)(jb + i) * ld + jb + j];
+        }
+        __syncthreads();
+        for (int j = bw - 1; j >= 1; j--) {
+            for (int idx = tid; idx < j * nrhs; idx += T) {
+                const int i = idx / nrhs, q = idx - i * nrhs;
+                Y[(jb + i) * nrhs + q] -= Ud[i * 33 + j] * Y[(jb + j) * nrhs + q];
+            }
+            __syncthreads();
+        }
+        for (int i = tid; i < jb; i += T) {
+            const double *row = A + (size_t)i * ld + jb;
+            double u[32];
+            for (int j = 0; j < bw; j++) u[j] = row[j];
+            for (int q = 0; q < nrhs; q++) {
+                double s = 0.0;
+                for (int j = 0; j < bw; j++) s = fma(u[j], Y[(jb + j) * nrhs + q], s);
+                Y[i * nrhs + q] -= s;
+            }
+        }
+        __syncthreads();
+    }
+    for (int idx = tid; idx < n * nrhs; idx += T) {
+        const int r = idx / nrhs, q = idx - r * nrhs;
+        A[(size_t)r * ld + n + q] = Y[idx];
+    }
+    if (tid == 0) *info = first_zero;
+}
+
+__global__ void batch_lu_kernel(double *data, const BatchSys *sys, const int *order, int count, int *counter,
+                                int *info, int pw, long smem_doubles)
+{
+    extern __shared__ double bsm[];
+    __shared__ double s_v[32];
+    __shared__ int s_i[32];
+    __shared__ int s_next;
+    __shared__ int s_piv[64];
+    __shared__ double s_dinv[64];
+    for (;;) {
+        if (threadIdx.x == 0) s_next = atomicAdd(counter, 1);
+        __syncthreads();
+        const int q = s_next;
+        __syncthreads();
+        if (q >= count) break;
+        const int i = order[q];
+        const BatchSys S = sys[i];
+        double *A = data + S.off;
+        if ((long)S.n * (S.n + S.nrhs) <= smem_doubles) {
+            batch_solve_smem(A, S.ld, S.n, S.nrhs, bsm, info + i, s_v, s_i);
+        } else {
+            // panel (n x pw) then the U chunk (pw x 64)
+            batch_solve_blocked(A, S.ld, S.n, S.nrhs, pw, bsm, bsm + (size_t)S.n * pw, s_piv, s_dinv, info + i, s_v,
+                                s_i);
+        }
+        __syncthreads();
+    }
+}
+
+long batch_smem_doubles(const BatchSys *sys, int count, int pw)
+{
+    // blocked path of system i: its panel (n x pw) then either the U chunk
+    // (pw x 64) or, in the back substitution, y (n x nrhs) then a 32 x 33
+    // diagonal block; the in-shared-memory path uses whatever this leaves
+    long need = 0;
+    const long tail = pw * 64 > 32 * 33 ? pw * 64 : 32 * 33;
+    for (int i = 0; i < count; i++) {
+        const long w = sys[i].nrhs > pw ? sys[i].nrhs : pw;
+        const long ni = (long)sys[i].n * w + tail;
+        if (ni > need) need = ni;
+    }
+    return need;
+}
+
+cudaError_t batch_lu_grid(int threads, long smem_doubles, int ctas_per_sm, int count, int *grid)
+{
+    if (threads < 64 || threads > 1024 || (threads & 31)) return cudaErrorInvalidValue;
+    const size_t smem = (size_t)smem_doubles * sizeof(double);
+    if (smem > BATCH_SMEM_MAX) return cudaErrorInvalidValue;
+    cudaError_t e = cudaFuncSetAttribute(batch_lu_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, BATCH_SMEM_MAX);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 148;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    int occ = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_lu_kernel, threads, smem)) != cudaSuccess)
+        return e;
+    if (occ < 1) return cudaErrorInvalidConfiguration;
+    if (ctas_per_sm > occ || ctas_per_sm < 1) ctas_per_sm = occ;
+    int g = sms * ctas_per_sm;
+    *grid = g > count ? count : g;
+    return cudaSuccess;
+}
+
+cudaError_t launch_batch_lu(double *data, const BatchSys *sys, const int *order, int count, int *counter, int *info,
+                            long smem_doubles, int pw, int threads, int grid, cudaStream_t st)
+{
+    if (count <= 0) return cudaSuccess;
+    if (pw < 16 || pw > 64 || threads < 64 || threads > 1024 || (threads & 31) || grid < 1 ||
+        (size_t)smem_doubles * sizeof(double) > BATCH_SMEM_MAX)
+        return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), st);
+    if (e != cudaSuccess) return e;
+    count_launch();
+    batch_lu_kernel<<<grid, threads, (size_t)smem_doubles * sizeof(double), st>>>(data, sys, order, count, counter,
+                                                                                   info, pw, smem_doubles);
+    return cudaGetLastError();
+}
+
+// HPL scaled residual of every solved system against its original copy:
+// out[i] = max over right-hand sides of ||A x - b||_inf / (eps (||A||_inf ||x||_inf + ||b||_inf) n)
+__global__ void batch_residual_kernel(const double *orig, const double *solved, const BatchSys *sys, int count,
+                                      double *out)
+{
+    __shared__ double s_r[32], s_a[32], s_x[32], s_b[32];
+    for (int i = blockIdx.x; i < count; i += gridDim.x) {
+        const BatchSys S = sys[i];
+        const double *A = orig + S.off, *X = solved + S.off;
+        double worst = 0.0;
+        for (int q = 0; q < S.nrhs; q++) {
+            double rmax = 0, amax = 0, xmax = 0, bmax = 0;
+            for (int r = threadIdx.x; r < S.n; r += blockDim.x) {
+                double s = 0, sa = 0;
+                for (int c = 0; c < S.n; c++) {
+                    const double a = A[(size_t)r * S.ld + c];
+                    s = fma(a, X[(size_t)c * S.ld + S.n + q], s);
+                    sa += fabs(a);
+                }
+                const double b = A[(size_t)r * S.ld + S.n + q];
+                rmax = fmax(rmax, fabs(s - b));
+                amax = fmax(amax, sa);
+                bmax = fmax(bmax, fabs(b));
+                xmax = fmax(xmax, fabs(X[(size_t)r * S.ld + S.n + q]));
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                rmax = fmax(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
+                amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+                xmax = fmax(xmax, __shfl_xor_sync(0xffffffffu, xmax, o));
+                bmax = fmax(bmax, __shfl_xor_sync(0xffffffffu, bmax, o));
+            }
+            const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+            if (lane == 0) {
+                s_r[warp] = rmax;
+                s_a[warp] = amax;
+                s_x[warp] = xmax;
+                s_b[warp] = bmax;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                for (int w2 = 1; w2 < nw; w2++) {
+                    rmax = fmax(rmax, s_r[w2]);
+                    amax = fmax(amax, s_a[w2]);
+                    xmax = fmax(xmax, s_x[w2]);
+                    bmax = fmax(bmax, s_b[w2]);
+                }
+                const double h = rmax / (1.1102230246251565e-16 * (amax * xmax + bmax) * S.n);
+                worst = fmax(worst, h);
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) out[i] = worst;
+    }
+}
+
+cudaError_t launch_batch_residual(const double *orig, const double *solved, const BatchSys *sys, int count,
+                                  double *out, cudaStream_t st)
+{
+    if (count <= 0) return cudaSuccess;
+    count_launch();
+    batch_residual_kernel<<<count < 148 * 8 ? count : 148 * 8, 256, 0, st>>>(orig, solved, sys, count, out);
+    return cudaGetLastError();
+}
+
+// system i of a batch: lu2's stream (randomsetmat) with seed base + i
+__global__ void batch_generate_kernel(double *data, const BatchSys *sys, int count, unsigned long long seed_base)
+{
+    for (int i = blockIdx.x; i < count; i += gridDim.x) {
+        const BatchSys S = sys[i];
+        double *A = data + S.off;
+        const unsigned long long xs = (((seed_base + i) & 0xffffffffull) << 16) | 0x330Eull;
+        const long total = (long)S.n * (S.n + 1) + (long)S.n * (S.nrhs - 1);
+        for (long q = threadIdx.x; q < total; q += blockDim.x) {
+            unsigned long long k = q + 1, aa = 1, cc = 0, ba = 0x5DEECE66Dull, bc = 0xBull;
+            const unsigned long long M = (1ull << 48) - 1;
+            while (k) {
+                if (k & 1) {
+                    cc = (ba * cc + bc) & M;
+                    aa = (ba * aa) & M;
+                }
+                bc = (ba * bc + bc) & M;
+                ba = (ba * ba) & M;
+                k >>= 1;
+            }
+            const double v = (double)((aa * xs + cc) & M) * (1.0 / 281474976710656.0) - 0.5;
+            long r, c;
+            if (q < (long)S.n * (S.n + 1)) {
+                r = q / (S.n + 1);
+                c = q - r * (S.n + 1);
+            } else {
+                const long e = q - (long)S.n * (S.n + 1);
+                c = S.n + 1 + e / S.n;
+                r = e % S.n;
+            }
+            A[(size_t)r * S.ld + c] = v;
+        }
+    }
+}
+
+cudaError_t launch_batch_generate(double *data, const BatchSys *sys, int count, unsigned long long seed_base,
+                                  cudaStream_t st)
+{
+    if (count <= 0) return cudaSuccess;
+    count_launch();
+    batch_generate_kernel<<<count < 148 * 16 ? count : 148 * 16, 256, 0, st>>>(data, sys, count, seed_base);
+    return cudaGetLastError();
+}
+
+}  // namespace lu2gpu

@@ -6,7 +6,9 @@
 // doneflag = 0, lu2gpu_last_error()) and, for the reference's void entry
 // points, ends the process like the reference's MP_error (lu2_mp_nompi.c:55-58)
 // unless lu2gpu_set_abort_on_error(0) was called.
+#include <algorithm>
 #include <atomic>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -163,6 +165,12 @@ extern "C" int lu2gpu_create(lu2gpu_ctx **out, int device)
     c->own_stream = true;
     c->leaf_ctas = leaf_max_ctas(device);
     const int G = c->leaf_ctas;
+    // the leaf may use fewer CTAs than fit (fewer participants per column
+    // exchange, more rows each): LU2GPU_LEAF_CTAS caps it
+    if (const char *e = getenv("LU2GPU_LEAF_CTAS")) {
+        const int cap = atoi(e);
+        if (cap >= 1 && cap < c->leaf_ctas) c->leaf_ctas = cap;
+    }
     size_t leaf_bytes = (size_t)2 * G * sizeof(LeafSlot);
     char *lb = nullptr;
     if (cudaMalloc(&c->d_status, 4 * sizeof(int)) != cudaSuccess || cudaMalloc(&lb, leaf_bytes) != cudaSuccess ||
@@ -924,6 +932,262 @@ extern "C" int lu2gpu_lumcolumn(int n, double *a, double *b, int m, int *pv, int
     return rc;
 }
 
+// ----- lu2.c per-panel entry points and lu2tlib.h's column-major slab API -----
+//
+// These take lu2's host arrays like the reference's functions and run the
+// same GPU kernels on a device copy of the region each call touches: rows
+// i..n-1 of the columns involved, as a view whose element (0,0) is global
+// (i, i) so that pivot rows and the reference-mode column parity stay global.
+
+// right part of a view with K = k1 - k0 not a multiple of 16 (the slab API's
+// inner blocks): exact-extent tensor maps zero-fill the GEMM's K remainder
+static int right_part_anyk(lu2gpu_ctx *c, const View &v, int k0, int k1, int cs, int ce)
+{
+    if (ce <= cs) return 0;
+    if ((k1 - k0) % 16 == 0) return right_part(c, v, k0, k1, cs, ce, false);
+    const int K = k1 - k0;
+    K_TRY(launch_laswp_scale(v.a, v.ld, k0, k1, c->d_ipiv + v.goff, v.goff, c->d_dinv + v.goff, cs, ce, true,
+                             c->stream));
+    K_TRY(launch_trsm_unit_lower(v.a, v.ld, k0, K, cs, ce, c->d_bt, c->stream));
+    if (k1 < v.n) {
+        const long ldk = (K + 1) & ~1L;
+        double *lk;
+        int rc = stage(c, 3, (size_t)(v.n - k1) * ldk, &lk);
+        if (rc) return rc;
+        // L21 (rows k1.., columns k0..k1) into an even-stride buffer, then C -= L21 U12
+        CU_TRY(cudaMemcpy2DAsync(lk, ldk * sizeof(double), v.a + (size_t)k1 * v.ld + k0, v.ld * sizeof(double),
+                                 (size_t)K * sizeof(double), v.n - k1, cudaMemcpyDeviceToDevice, c->stream));
+        K_TRY(launch_dgemm_general(lk, ldk, c->d_bt, K, v.a + (size_t)k1 * v.ld + cs, v.ld, v.n - k1, ce - cs, K, -1.0,
+                                   1.0, c->d_status, c->stream));
+    }
+    return 0;
+}
+
+// stage rows i..n-1, columns i..i+w-1 of lu2's a[n][rdim] into a device view
+static int stage_rows(lu2gpu_ctx *c, const double *a, long rdim, int n, int i, int w, int slot, View *v)
+{
+    const long ld = ((long)w + 15) & ~15L;
+    double *d;
+    int rc = stage(c, slot, (size_t)(n - i) * ld, &d);
+    if (rc) return rc;
+    CU_TRY(cudaMemcpy2DAsync(d, ld * sizeof(double), a + (size_t)i * rdim + i, rdim * sizeof(double),
+                             (size_t)w * sizeof(double), n - i, cudaMemcpyHostToDevice, c->stream));
+    *v = View{d, ld, n - i, w, i};
+    return 0;
+}
+
+static int unstage_rows(lu2gpu_ctx *c, double *a, long rdim, int i, int col0, int w, const View &v)
+{
+    CU_TRY(cudaMemcpy2DAsync(a + (size_t)i * rdim + i + col0, rdim * sizeof(double), v.a + col0, v.ld * sizeof(double),
+                             (size_t)w * sizeof(double), v.n, cudaMemcpyDeviceToHost, c->stream));
+    return 0;
+}
+
+// column_decomposition_recursive (lu2.c:1088-1120): the panel of columns
+// i..i+m-1, rows i..n-1, of a[n][n+16]; pv[0..m) = global pivot rows.
+static int colrec_host(int n, double *a, int m, int *pv, int i, int mode)
+{
+    lu2gpu_ctx *c = default_ctx();
+    if (!c) return LU2GPU_ERR_NODEV;
+    if (n <= 0 || !a || !pv || m <= 0 || i < 0 || i + m > n) {
+        set_error("column_decomposition_recursive: bad arguments (n=%d m=%d i=%d)", n, m, i);
+        return LU2GPU_ERR_ARG;
+    }
+    DeviceGuard g(c->device);
+    // the recursion's inner right parts hold a K x (m - K) transposed U block
+    int rc = ensure_work(c, n, m + 16, m);
+    if (rc) return rc;
+    if ((rc = begin_status(c))) return rc;
+    View v;
+    if ((rc = stage_rows(c, a, (long)n + 16, n, i, m, 0, &v))) return rc;
+    if ((rc = panel(c, v, 0, m, mode))) return rc;
+    if ((rc = unstage_rows(c, a, (long)n + 16, i, 0, m, v))) return rc;
+    CU_TRY(cudaMemcpyAsync(pv, c->d_ipiv + i, (size_t)m * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    return end_status(c, "column_decomposition_recursive");
+}
+
+// caller-supplied pivot rows: pv[k] must name a row of the trailing block
+// (i + k <= pv[k] < n), as lu2's pivot search produces them
+static bool pivots_valid(const int *pv, int m, int i, int n, const char *who)
+{
+    for (int k = 0; k < m; k++)
+        if (pv[k] < i + k || pv[k] >= n) {
+            set_error("%s: pivot %d is row %d (must be in [%d, %d))", who, k, pv[k], i + k, n);
+            return false;
+        }
+    return true;
+}
+
+// process_right_part (lu2.c:524-581): pivots pv[0..m) of rows i..i+m-1 applied
+// to columns i+m..iend-1 with the 1/pivot scaling, U block solved, rows
+// i+m..n-1 updated.
+static int rightpart_host(int n, double *a, int m, const int *pv, int i, int iend)
+{
+    lu2gpu_ctx *c = default_ctx();
+    if (!c) return LU2GPU_ERR_NODEV;
+    if (n <= 0 || !a || !pv || m <= 0 || i < 0 || i + m > n || iend < i + m || iend > n + 16) {
+        set_error("process_right_part: bad arguments (n=%d m=%d i=%d iend=%d)", n, m, i, iend);
+        return LU2GPU_ERR_ARG;
+    }
+    if (!pivots_valid(pv, m, i, n, "process_right_part")) return LU2GPU_ERR_ARG;
+    DeviceGuard g(c->device);
+    int rc = ensure_work(c, n, iend - i + 16, m);
+    if (rc) return rc;
+    if ((rc = begin_status(c))) return rc;
+    View v;
+    if ((rc = stage_rows(c, a, (long)n + 16, n, i, iend - i, 0, &v))) return rc;
+    CU_TRY(cudaMemcpyAsync(c->d_ipiv + i, pv, (size_t)m * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    K_TRY(launch_diag_inv(v.a, v.ld, m, c->d_dinv + i, c->stream));
+    if ((rc = right_part_anyk(c, v, 0, m, m, iend - i))) return rc;
+    if ((rc = unstage_rows(c, a, (long)n + 16, i, m, iend - i - m, v))) return rc;
+    return end_status(c, "process_right_part");
+}
+
+// backward_sub (lu2.c:110-116): b = U'^{-1} (column n) with a's unit upper factor
+static int backsub_host(int n, const double *a, double *b)
+{
+    lu2gpu_ctx *c = default_ctx();
+    if (!c) return LU2GPU_ERR_NODEV;
+    if (n <= 0 || !a || !b) {
+        set_error("backward_sub: bad arguments");
+        return LU2GPU_ERR_ARG;
+    }
+    DeviceGuard g(c->device);
+    const long rdim = (long)n + 16, ld = ((long)n + 16 + 1) & ~1L;
+    double *d, *x;
+    int rc;
+    if ((rc = stage(c, 0, (size_t)n * ld, &d)) || (rc = stage(c, 1, (size_t)n, &x))) return rc;
+    if ((rc = begin_status(c))) return rc;
+    CU_TRY(cudaMemcpy2DAsync(d, ld * sizeof(double), a, rdim * sizeof(double), (size_t)(n + 1) * sizeof(double), n,
+                             cudaMemcpyHostToDevice, c->stream));
+    CU_TRY(cudaMemcpy2DAsync(x, sizeof(double), d + n, ld * sizeof(double), sizeof(double), n,
+                             cudaMemcpyDeviceToDevice, c->stream));
+    K_TRY(launch_backsolve(d, ld, n, 1, x, 1, c->stream));
+    CU_TRY(cudaMemcpyAsync(b, x, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    return end_status(c, "backward_sub");
+}
+
+extern "C" void column_decomposition_recursive(int n, double *a, int m, double *awork, int *pv, int i)
+{
+    (void)awork;
+    if (colrec_host(n, a, m, pv, i, g_pivot_mode) < 0) fail_void("column_decomposition_recursive");
+}
+
+extern "C" void process_right_part(int n, double *a, int m, double *awork, int *pv, int i, int iend)
+{
+    (void)awork;
+    if (rightpart_host(n, a, m, pv, i, iend) < 0) fail_void("process_right_part");
+}
+
+extern "C" void backward_sub(int n, double *a, double *b)
+{
+    if (backsub_host(n, a, b) < 0) fail_void("backward_sub");
+}
+
+// The column-major slab of lu2tlib.c: a[j][r] at a + j*n + r (column stride
+// n), columns 0..m-1 relative to a (or 0..iend-i-1), rows i..n-1.  Staged
+// transposed into a row-major device view.
+static int stage_slab(lu2gpu_ctx *c, const double *a, int n, int i, int cols, View *v)
+{
+    const int rows = n - i;
+    const long ld = ((long)cols + 15) & ~15L, ldt = ((long)rows + 1) & ~1L;
+    double *d, *t;
+    int rc;
+    if ((rc = stage(c, 0, (size_t)rows * ld, &d)) || (rc = stage(c, 2, (size_t)cols * ldt, &t))) return rc;
+    CU_TRY(cudaMemcpy2DAsync(t, ldt * sizeof(double), a + i, (size_t)n * sizeof(double), (size_t)rows * sizeof(double),
+                             cols, cudaMemcpyHostToDevice, c->stream));
+    K_TRY(launch_transpose(t, ldt, d, ld, cols, rows, c->stream));
+    *v = View{d, ld, rows, cols, i};
+    return 0;
+}
+
+static int unstage_slab(lu2gpu_ctx *c, double *a, int n, int i, int col0, int cols, const View &v)
+{
+    const int rows = n - i;
+    const long ldt = ((long)rows + 1) & ~1L;
+    double *t;
+    int rc = stage(c, 2, (size_t)(col0 + cols) * ldt, &t);
+    if (rc) return rc;
+    K_TRY(launch_transpose(v.a + col0, v.ld, t, ldt, rows, cols, c->stream));
+    CU_TRY(cudaMemcpy2DAsync(a + (size_t)col0 * n + i, (size_t)n * sizeof(double), t, ldt * sizeof(double),
+                             (size_t)rows * sizeof(double), cols, cudaMemcpyDeviceToHost, c->stream));
+    return 0;
+}
+
+static int cm_decomp_host(int n, double *a, int m, int *pv, int i, bool recursive)
+{
+    lu2gpu_ctx *c = default_ctx();
+    if (!c) return LU2GPU_ERR_NODEV;
+    if (n <= 0 || !a || !pv || m <= 0 || i < 0 || i + m > n) {
+        set_error("cm_column_decomposition: bad arguments (n=%d m=%d i=%d)", n, m, i);
+        return LU2GPU_ERR_ARG;
+    }
+    int mode = g_pivot_mode;
+    if (!recursive) {
+        // column_decomposition (lu2tlib.c:1041-1066) called on the whole slab:
+        // in the reference's pivot search every column searches column 0
+        if (m > 16) {
+            set_error("cm_column_decomposition: slab of %d columns (at most 16)", m);
+            return LU2GPU_ERR_ARG;
+        }
+        if (mode == LU2GPU_PIVOT_REF) mode = PIVOT_REF_FIRST;
+    }
+    DeviceGuard g(c->device);
+    int rc = ensure_work(c, n, m + 16, m < 16 ? 16 : m);
+    if (rc) return rc;
+    if ((rc = begin_status(c))) return rc;
+    View v;
+    if ((rc = stage_slab(c, a, n, i, m, &v))) return rc;
+    if (recursive) {
+        if ((rc = panel(c, v, 0, m, mode))) return rc;
+    } else {
+        K_TRY(launch_leaf(v.a, v.ld, v.n, 0, m, mode, v.goff, c->d_ipiv + v.goff, c->d_dinv + v.goff, c->leaf,
+                          c->d_status, c->leaf_ctas, c->stream));
+    }
+    if ((rc = unstage_slab(c, a, n, i, 0, m, v))) return rc;
+    CU_TRY(cudaMemcpyAsync(pv, c->d_ipiv + i, (size_t)m * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    return end_status(c, "cm_column_decomposition");
+}
+
+extern "C" void cm_column_decomposition_recursive(int n, double *a, int m, int *pv, int i)
+{
+    if (cm_decomp_host(n, a, m, pv, i, true) < 0) fail_void("cm_column_decomposition_recursive");
+}
+
+extern "C" void cm_column_decomposition(int n, double *a, int m, int *pv, int i)
+{
+    if (cm_decomp_host(n, a, m, pv, i, false) < 0) fail_void("cm_column_decomposition");
+}
+
+// process_right_part of the slab (lu2tlib.c:1068-1093): columns m..iend-i-1
+static int cm_right_host(int n, double *a, int m, const int *pv, int i, int iend)
+{
+    lu2gpu_ctx *c = default_ctx();
+    if (!c) return LU2GPU_ERR_NODEV;
+    if (n <= 0 || !a || !pv || m <= 0 || i < 0 || i + m > n || iend < i + m || iend - i > n + 1) {
+        set_error("cm_process_right_part: bad arguments (n=%d m=%d i=%d iend=%d)", n, m, i, iend);
+        return LU2GPU_ERR_ARG;
+    }
+    if (!pivots_valid(pv, m, i, n, "cm_process_right_part")) return LU2GPU_ERR_ARG;
+    DeviceGuard g(c->device);
+    const int cols = iend - i;
+    int rc = ensure_work(c, n, cols + 16, ((m + 15) / 16) * 16);
+    if (rc) return rc;
+    if ((rc = begin_status(c))) return rc;
+    View v;
+    if ((rc = stage_slab(c, a, n, i, cols, &v))) return rc;
+    CU_TRY(cudaMemcpyAsync(c->d_ipiv + i, pv, (size_t)m * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    K_TRY(launch_diag_inv(v.a, v.ld, m, c->d_dinv + i, c->stream));
+    if ((rc = right_part_anyk(c, v, 0, m, m, cols))) return rc;
+    if ((rc = unstage_slab(c, a, n, i, m, cols - m, v))) return rc;
+    return end_status(c, "cm_process_right_part");
+}
+
+extern "C" void cm_process_right_part(int n, double *a, int m, int *pv, int i, int iend)
+{
+    if (cm_right_host(n, a, m, pv, i, iend) < 0) fail_void("cm_process_right_part");
+}
+
 extern "C" int lu2gpu_copy_pivots(lu2gpu_ctx *c, int *ipiv_host, int n)
 {
     if (!c || !ipiv_host || n <= 0 || (size_t)n > c->piv_cap) {
@@ -1205,6 +1469,315 @@ extern "C" int lu2gpu_bf16_update_dev(lu2gpu_ctx *c, int M, int N, int K, const 
     CU_TRY(cudaMemcpyAsync(dscale, &scale, sizeof(float), cudaMemcpyHostToDevice, c->stream));
     K_TRY(launch_bf16_update(a16, lda, bt16, ldb, c32, ldc, M, N, K, dscale, c->d_status, c->stream));
     return end_status(c, "lu2gpu_bf16_update_dev");
+}
+
+// ---------------------------------------------------------------------------
+// Batching form: many independent systems of uneven order in one persistent
+// launch (kernels_batch.cu), replayed from a CUDA graph.
+
+struct lu2gpu_batch {
+    lu2gpu_ctx *ctx = nullptr;
+    int count = 0, max_n = 0;
+    std::vector<BatchSys> sys;
+    BatchSys *d_sys = nullptr;
+    int *d_order = nullptr, *d_counter = nullptr, *d_info = nullptr;
+    double *d_data = nullptr, *d_orig = nullptr, *d_resid = nullptr;
+    size_t total = 0;  // doubles
+    int threads = 256, pw = 32, ctas_per_sm = 1;
+    long smem_doubles = 0;
+    int grid = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+static void batch_drop_graph(lu2gpu_batch *b)
+{
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+}
+
+// adopt a launch shape if every system of the batch fits it; 0 or an error status
+static int batch_configure(lu2gpu_batch *b, int threads, int pw, int ctas_per_sm)
+{
+    const long sd = batch_smem_doubles(b->sys.data(), b->count, pw);
+    if ((size_t)sd * sizeof(double) > BATCH_SMEM_MAX) {
+        set_error("batch: panel width %d needs %ld bytes of shared memory for n=%d (limit %zu)", pw,
+                  sd * (long)sizeof(double), b->max_n, BATCH_SMEM_MAX);
+        return LU2GPU_ERR_ARG;
+    }
+    int grid = 0;
+    cudaError_t e = batch_lu_grid(threads, sd, ctas_per_sm, b->count, &grid);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        set_error("batch: launch shape threads=%d pw=%d ctas=%d not launchable: %s", threads, pw, ctas_per_sm,
+                  cudaGetErrorString(e));
+        return LU2GPU_ERR_ARG;
+    }
+    b->threads = threads;
+    b->pw = pw;
+    b->ctas_per_sm = ctas_per_sm;
+    b->smem_doubles = sd;
+    b->grid = grid;
+    batch_drop_graph(b);
+    return 0;
+}
+
+extern "C" int lu2gpu_batch_destroy(lu2gpu_batch *b)
+{
+    if (!b) return 0;
+    DeviceGuard g(b->ctx->device);
+    cudaStreamSynchronize(b->ctx->stream);
+    batch_drop_graph(b);
+    cudaFree(b->d_sys);
+    cudaFree(b->d_order);
+    cudaFree(b->d_counter);
+    cudaFree(b->d_info);
+    cudaFree(b->d_data);
+    cudaFree(b->d_orig);
+    cudaFree(b->d_resid);
+    delete b;
+    return 0;
+}
+
+extern "C" int lu2gpu_batch_create(lu2gpu_ctx *c, int count, const int *n, const int *nrhs, lu2gpu_batch **out)
+{
+    if (!c || count <= 0 || !n || !out) {
+        set_error("lu2gpu_batch_create: bad arguments");
+        return LU2GPU_ERR_ARG;
+    }
+    *out = nullptr;
+    lu2gpu_batch *b = new lu2gpu_batch();
+    b->ctx = c;
+    b->count = count;
+    b->sys.resize(count);
+    size_t off = 0;
+    for (int i = 0; i < count; i++) {
+        const int ni = n[i], ri = nrhs ? nrhs[i] : 1;
+        if (ni < 1 || ni > 4096 || ri < 1 || ri > 64) {
+            delete b;
+            set_error("lu2gpu_batch_create: system %d has n=%d nrhs=%d (1 <= n <= 4096, 1 <= nrhs <= 64)", i, ni, ri);
+            return LU2GPU_ERR_ARG;
+        }
+        const int ld = (ni + ri + 1) & ~1;
+        b->sys[i] = BatchSys{(long long)off, ni, ri, ld, 0};
+        off += ((size_t)ni * ld + 1) & ~(size_t)1;  // every system starts 16-byte aligned
+        if (ni > b->max_n) b->max_n = ni;
+    }
+    b->total = off;
+    std::vector<int> order(count);
+    for (int i = 0; i < count; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return b->sys[x].n > b->sys[y].n; });
+    DeviceGuard g(c->device);
+    if (cudaMalloc(&b->d_sys, sizeof(BatchSys) * count) != cudaSuccess ||
+        cudaMalloc(&b->d_order, sizeof(int) * count) != cudaSuccess ||
+        cudaMalloc(&b->d_counter, sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&b->d_info, sizeof(int) * count) != cudaSuccess ||
+        cudaMalloc(&b->d_resid, sizeof(double) * count) != cudaSuccess ||
+        cudaMalloc(&b->d_data, sizeof(double) * b->total) != cudaSuccess) {
+        cudaGetLastError();
+        lu2gpu_batch_destroy(b);
+        set_error("lu2gpu_batch_create: device allocation of %zu bytes failed", sizeof(double) * off);
+        return LU2GPU_ERR_NOMEM;
+    }
+    int rc = 0;
+    if (cudaMemcpy(b->d_sys, b->sys.data(), sizeof(BatchSys) * count, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(b->d_order, order.data(), sizeof(int) * count, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(b->d_data, 0, sizeof(double) * b->total) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("lu2gpu_batch_create: device copy failed");
+        rc = LU2GPU_ERR_CUDA;
+    } else if (batch_configure(b, 256, 32, 1) != 0) {
+        rc = batch_configure(b, 256, 16, 1);  // default panel width 32, 16 for larger systems
+    }
+    if (rc) {
+        lu2gpu_batch_destroy(b);
+        return rc;
+    }
+    *out = b;
+    return 0;
+}
+
+extern "C" int lu2gpu_batch_system(lu2gpu_batch *b, int i, double **a, long *ld)
+{
+    if (!b || i < 0 || i >= b->count) {
+        set_error("lu2gpu_batch_system: bad index");
+        return LU2GPU_ERR_ARG;
+    }
+    if (a) *a = b->d_data + b->sys[i].off;
+    if (ld) *ld = b->sys[i].ld;
+    return 0;
+}
+
+extern "C" int lu2gpu_batch_generate(lu2gpu_batch *b, long seed)
+{
+    if (!b) return LU2GPU_ERR_ARG;
+    DeviceGuard g(b->ctx->device);
+    K_TRY(launch_batch_generate(b->d_data, b->d_sys, b->count, (unsigned long long)seed, b->ctx->stream));
+    CU_TRY(cudaStreamSynchronize(b->ctx->stream));
+    return 0;
+}
+
+extern "C" int lu2gpu_batch_snapshot(lu2gpu_batch *b)
+{
+    if (!b) return LU2GPU_ERR_ARG;
+    DeviceGuard g(b->ctx->device);
+    if (!b->d_orig && cudaMalloc(&b->d_orig, sizeof(double) * b->total) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("lu2gpu_batch_snapshot: allocation failed");
+        return LU2GPU_ERR_NOMEM;
+    }
+    CU_TRY(cudaMemcpyAsync(b->d_orig, b->d_data, sizeof(double) * b->total, cudaMemcpyDeviceToDevice,
+                           b->ctx->stream));
+    CU_TRY(cudaStreamSynchronize(b->ctx->stream));
+    return 0;
+}
+
+extern "C" int lu2gpu_batch_restore(lu2gpu_batch *b)
+{
+    if (!b || !b->d_orig) {
+        set_error("lu2gpu_batch_restore: no snapshot");
+        return LU2GPU_ERR_ARG;
+    }
+    DeviceGuard g(b->ctx->device);
+    CU_TRY(cudaMemcpyAsync(b->d_data, b->d_orig, sizeof(double) * b->total, cudaMemcpyDeviceToDevice,
+                           b->ctx->stream));
+    return 0;
+}
+
+static int batch_enqueue(lu2gpu_batch *b)
+{
+    K_TRY(launch_batch_lu(b->d_data, b->d_sys, b->d_order, b->count, b->d_counter, b->d_info, b->smem_doubles, b->pw,
+                          b->threads, b->grid, b->ctx->stream));
+    return 0;
+}
+
+extern "C" int lu2gpu_batch_set_config(lu2gpu_batch *b, int threads, int pw, int ctas_per_sm)
+{
+    if (!b || threads < 64 || threads > 1024 || (threads & 31) || pw < 16 || pw > 64 || ctas_per_sm < 1) {
+        set_error("lu2gpu_batch_set_config: threads in [64,1024] (multiple of 32), pw in [16,64], ctas >= 1");
+        return LU2GPU_ERR_ARG;
+    }
+    DeviceGuard g(b->ctx->device);
+    return batch_configure(b, threads, pw, ctas_per_sm);
+}
+
+// Factor and solve every system in place; the launch is captured into a CUDA
+// graph on the first call with the current configuration and replayed after.
+extern "C" int lu2gpu_batch_solve(lu2gpu_batch *b, int *info_host)
+{
+    if (!b) return LU2GPU_ERR_ARG;
+    DeviceGuard g(b->ctx->device);
+    cudaStream_t st = b->ctx->stream;
+    if (!b->exec) {
+        if (!st) {
+            set_error("lu2gpu_batch_solve: needs a non-default stream to capture its graph");
+            return LU2GPU_ERR_ARG;
+        }
+        CU_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        int rc = batch_enqueue(b);
+        cudaGraph_t gr = nullptr;
+        cudaError_t e = cudaStreamEndCapture(st, &gr);
+        if (rc) {
+            if (gr) cudaGraphDestroy(gr);
+            return rc;
+        }
+        CU_TRY(e);
+        b->graph = gr;
+        CU_TRY(cudaGraphInstantiate(&b->exec, b->graph, 0));
+    }
+    CU_TRY(cudaGraphLaunch(b->exec, st));
+    CU_TRY(cudaStreamSynchronize(st));
+    if (info_host) CU_TRY(cudaMemcpy(info_host, b->d_info, sizeof(int) * b->count, cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+// Time the persistent launch over launch shapes (threads per CTA, panel width,
+// CTAs per SM) on this batch's own data (restored from a snapshot before every
+// trial) and keep the fastest; params_out = {threads, pw, ctas_per_sm, best us}.
+extern "C" int lu2gpu_batch_autotune(lu2gpu_batch *b, int *params_out)
+{
+    if (!b) return LU2GPU_ERR_ARG;
+    DeviceGuard g(b->ctx->device);
+    int rc = lu2gpu_batch_snapshot(b);
+    if (rc) return rc;
+    cudaStream_t st = b->ctx->stream;
+    const int cand_threads[3] = {128, 256, 512}, cand_pw[3] = {16, 32, 64}, cand_ctas[2] = {1, 2};
+    float best = 1e30f;
+    int bt = b->threads, bp = b->pw, bc = b->ctas_per_sm;
+    cudaEvent_t e0, e1;
+    CU_TRY(cudaEventCreate(&e0));
+    CU_TRY(cudaEventCreate(&e1));
+    for (int ti = 0; ti < 3; ti++)
+        for (int pi = 0; pi < 3; pi++)
+            for (int ci = 0; ci < 2; ci++) {
+                if (batch_configure(b, cand_threads[ti], cand_pw[pi], cand_ctas[ci])) continue;  // does not fit
+                if ((rc = lu2gpu_batch_restore(b))) return rc;
+                CU_TRY(cudaEventRecord(e0, st));
+                if ((rc = batch_enqueue(b))) return rc;
+                CU_TRY(cudaEventRecord(e1, st));
+                CU_TRY(cudaEventSynchronize(e1));
+                float ms = 0;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (ms < best) {
+                    best = ms;
+                    bt = b->threads;
+                    bp = b->pw;
+                    bc = b->ctas_per_sm;
+                }
+            }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if ((rc = batch_configure(b, bt, bp, bc))) return rc;
+    if ((rc = lu2gpu_batch_restore(b))) return rc;
+    CU_TRY(cudaStreamSynchronize(st));
+    if (params_out) {
+        params_out[0] = bt;
+        params_out[1] = bp;
+        params_out[2] = bc;
+        params_out[3] = (int)(best * 1000.f);
+    }
+    return 0;
+}
+
+extern "C" int lu2gpu_batch_residuals(lu2gpu_batch *b, double *out_host)
+{
+    if (!b || !b->d_orig || !out_host) {
+        set_error("lu2gpu_batch_residuals: needs a snapshot of the original systems");
+        return LU2GPU_ERR_ARG;
+    }
+    DeviceGuard g(b->ctx->device);
+    K_TRY(launch_batch_residual(b->d_orig, b->d_data, b->d_sys, b->count, b->d_resid, b->ctx->stream));
+    CU_TRY(cudaStreamSynchronize(b->ctx->stream));
+    CU_TRY(cudaMemcpy(out_host, b->d_resid, sizeof(double) * b->count, cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+// The batch of the benchmark: n_i log-uniform in [nmin, nmax] and, for a
+// fraction frac_multi of the systems, nrhs_multi right-hand sides (else one),
+// from the 48-bit drand48 stream seeded with `seed`.
+extern "C" int lu2gpu_batch_sizes(int count, long seed, int nmin, int nmax, double frac_multi, int nrhs_multi,
+                                  int *n_out, int *nrhs_out)
+{
+    if (count <= 0 || nmin < 1 || nmax < nmin || !n_out || !nrhs_out) {
+        set_error("lu2gpu_batch_sizes: bad arguments");
+        return LU2GPU_ERR_ARG;
+    }
+    unsigned long long x = ((((unsigned long long)seed) & 0xffffffffull) << 16) | 0x330Eull;
+    auto next = [&]() {
+        x = (0x5DEECE66Dull * x + 0xBull) & ((1ull << 48) - 1);
+        return (double)x * (1.0 / 281474976710656.0);
+    };
+    const double l0 = log((double)nmin), l1 = log((double)nmax + 1.0);
+    for (int i = 0; i < count; i++) {
+        int ni = (int)floor(exp(l0 + next() * (l1 - l0)));
+        if (ni < nmin) ni = nmin;
+        if (ni > nmax) ni = nmax;
+        n_out[i] = ni;
+        nrhs_out[i] = (next() < frac_multi) ? nrhs_multi : 1;
+    }
+    return 0;
 }
 
 // lumcolumn's panel loop (lu2.c:1126-1141) on the FP32 working matrix

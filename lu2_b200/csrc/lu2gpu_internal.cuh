@@ -174,6 +174,30 @@ cudaError_t launch_f32_transpose_bf16(const float *u, long ld, int K, int N, voi
                                       cudaStream_t st);
 // x += (double) d
 cudaError_t launch_add_f32_to_f64(const float *d, double *x, int n, cudaStream_t st);
+
+// ---------------------------------------------------------------------------
+// batching form (kernels_batch.cu)
+
+// one system of a batch: its augmented matrix (n x (n+nrhs), row stride ld)
+// starts at data + off
+struct BatchSys {
+    long long off;
+    int n, nrhs, ld, pad_;
+};
+// dynamic shared memory a CTA of the batched launch may use
+constexpr size_t BATCH_SMEM_MAX = 220 * 1024;
+// shared-memory doubles a CTA needs for the systems sys[0..count) with panel width pw
+long batch_smem_doubles(const BatchSys *sys, int count, int pw);
+// persistent grid for a launch shape (sets the kernel's shared-memory limit;
+// call outside stream capture)
+cudaError_t batch_lu_grid(int threads, long smem_doubles, int ctas_per_sm, int count, int *grid);
+// factor + solve every system, CTAs pulling systems in `order` from `counter`
+cudaError_t launch_batch_lu(double *data, const BatchSys *sys, const int *order, int count, int *counter, int *info,
+                            long smem_doubles, int pw, int threads, int grid, cudaStream_t st);
+cudaError_t launch_batch_residual(const double *orig, const double *solved, const BatchSys *sys, int count,
+                                  double *out, cudaStream_t st);
+cudaError_t launch_batch_generate(double *data, const BatchSys *sys, int count, unsigned long long seed_base,
+                                  cudaStream_t st);
 // *out = max(*out, max |v|) as double bits
 cudaError_t launch_vec_absmax(const double *v, int n, unsigned long long *out, cudaStream_t st);
 

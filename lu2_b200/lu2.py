@@ -196,6 +196,73 @@ class Context:
         return {TIMER_NAMES[i]: (float(ms[i]), int(cnt[i])) for i in range(k)}
 
 
+def batch_sizes(count: int, seed: int, nmin: int = 16, nmax: int = 512, frac_multi: float = 0.1,
+                nrhs_multi: int = 8):
+    """Orders log-uniform in [nmin, nmax]; a fraction frac_multi get nrhs_multi right-hand sides."""
+    n = np.zeros(count, dtype=np.int32)
+    r = np.zeros(count, dtype=np.int32)
+    _check("lu2gpu_batch_sizes", lib().lu2gpu_batch_sizes(count, seed, nmin, nmax, frac_multi, nrhs_multi,
+                                                          _ptr(n), _ptr(r)))
+    return n, r
+
+
+class Batch:
+    """A batch of independent systems solved by one persistent launch."""
+
+    def __init__(self, ctx: Context, n, nrhs=None):
+        self.n = np.ascontiguousarray(n, dtype=np.int32)
+        self.nrhs = np.ascontiguousarray(nrhs if nrhs is not None else np.ones_like(self.n), dtype=np.int32)
+        self.count = len(self.n)
+        self._h = C.c_void_p()
+        _check("lu2gpu_batch_create", lib().lu2gpu_batch_create(ctx.handle, self.count, _ptr(self.n),
+                                                                _ptr(self.nrhs), C.byref(self._h)))
+
+    def close(self) -> None:
+        if self._h:
+            lib().lu2gpu_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def system(self, i: int):
+        """(device pointer, row stride) of system i's augmented matrix."""
+        p = C.c_void_p()
+        ld = C.c_long()
+        _check("lu2gpu_batch_system", lib().lu2gpu_batch_system(self._h, i, C.byref(p), C.byref(ld)))
+        return p.value, ld.value
+
+    def generate(self, seed: int) -> None:
+        _check("lu2gpu_batch_generate", lib().lu2gpu_batch_generate(self._h, seed))
+
+    def snapshot(self) -> None:
+        _check("lu2gpu_batch_snapshot", lib().lu2gpu_batch_snapshot(self._h))
+
+    def restore(self) -> None:
+        _check("lu2gpu_batch_restore", lib().lu2gpu_batch_restore(self._h))
+
+    def set_config(self, threads: int, pw: int, ctas_per_sm: int) -> None:
+        _check("lu2gpu_batch_set_config", lib().lu2gpu_batch_set_config(self._h, threads, pw, ctas_per_sm))
+
+    def autotune(self) -> dict:
+        out = np.zeros(4, dtype=np.int32)
+        _check("lu2gpu_batch_autotune", lib().lu2gpu_batch_autotune(self._h, _ptr(out)))
+        return {"threads": int(out[0]), "pw": int(out[1]), "ctas_per_sm": int(out[2]), "us": int(out[3])}
+
+    def solve(self) -> np.ndarray:
+        info = np.zeros(self.count, dtype=np.int32)
+        _check("lu2gpu_batch_solve", lib().lu2gpu_batch_solve(self._h, _ptr(info)))
+        return info
+
+    def residuals(self) -> np.ndarray:
+        out = np.zeros(self.count, dtype=np.float64)
+        _check("lu2gpu_batch_residuals", lib().lu2gpu_batch_residuals(self._h, _ptr(out)))
+        return out
+
+
 def device_ld(n: int, nrhs: int = 1) -> int:
     """A row stride for device matrices: >= n + nrhs, even, 128-byte rows."""
     return ((n + nrhs + 15) // 16) * 16

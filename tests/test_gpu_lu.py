@@ -190,7 +190,7 @@ def test_pivot_ties_go_to_lowest_row(ctx, oracle):
 @pytest.mark.skipif(not RefLib.available("fixed"), reason="compiled reference not present")
 @pytest.mark.parametrize("variant,mode", [("fixed", PIVOT_PARTIAL), ("shipped", PIVOT_REF)])
 def test_n8192_against_compiled_reference(ctx, oracle, variant, mode):
-    """configs[1]'s cross-check: the reference CPU lu2 at N=8192 on identical inputs."""
+    """Cross-check at N=8192 (nb=256): the compiled reference CPU lu2 on identical inputs."""
     import os
 
     n, nb, seed = 8192, 256, 1
