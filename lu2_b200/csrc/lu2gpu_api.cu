@@ -1486,6 +1486,7 @@ struct lu2gpu_batch {
     int threads = 256, pw = 32, ctas_per_sm = 1;
     long smem_doubles = 0;
     int grid = 0;
+    cudaStream_t capture = nullptr;  // private stream the graph is captured on
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
 };
@@ -1537,6 +1538,7 @@ extern "C" int lu2gpu_batch_destroy(lu2gpu_batch *b)
     cudaFree(b->d_data);
     cudaFree(b->d_orig);
     cudaFree(b->d_resid);
+    if (b->capture) cudaStreamDestroy(b->capture);
     delete b;
     return 0;
 }
@@ -1575,7 +1577,8 @@ extern "C" int lu2gpu_batch_create(lu2gpu_ctx *c, int count, const int *n, const
         cudaMalloc(&b->d_counter, sizeof(int)) != cudaSuccess ||
         cudaMalloc(&b->d_info, sizeof(int) * count) != cudaSuccess ||
         cudaMalloc(&b->d_resid, sizeof(double) * count) != cudaSuccess ||
-        cudaMalloc(&b->d_data, sizeof(double) * b->total) != cudaSuccess) {
+        cudaMalloc(&b->d_data, sizeof(double) * b->total) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->capture, cudaStreamNonBlocking) != cudaSuccess) {
         cudaGetLastError();
         lu2gpu_batch_destroy(b);
         set_error("lu2gpu_batch_create: device allocation of %zu bytes failed", sizeof(double) * off);
@@ -1646,10 +1649,10 @@ extern "C" int lu2gpu_batch_restore(lu2gpu_batch *b)
     return 0;
 }
 
-static int batch_enqueue(lu2gpu_batch *b)
+static int batch_enqueue(lu2gpu_batch *b, cudaStream_t st)
 {
     K_TRY(launch_batch_lu(b->d_data, b->d_sys, b->d_order, b->count, b->d_counter, b->d_info, b->smem_doubles, b->pw,
-                          b->threads, b->grid, b->ctx->stream));
+                          b->threads, b->grid, st));
     return 0;
 }
 
@@ -1671,14 +1674,12 @@ extern "C" int lu2gpu_batch_solve(lu2gpu_batch *b, int *info_host)
     DeviceGuard g(b->ctx->device);
     cudaStream_t st = b->ctx->stream;
     if (!b->exec) {
-        if (!st) {
-            set_error("lu2gpu_batch_solve: needs a non-default stream to capture its graph");
-            return LU2GPU_ERR_ARG;
-        }
-        CU_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        int rc = batch_enqueue(b);
+        // captured on the batch's own stream (the context's may be the legacy
+        // default stream, which cannot be captured), launched on the context's
+        CU_TRY(cudaStreamBeginCapture(b->capture, cudaStreamCaptureModeThreadLocal));
+        int rc = batch_enqueue(b, b->capture);
         cudaGraph_t gr = nullptr;
-        cudaError_t e = cudaStreamEndCapture(st, &gr);
+        cudaError_t e = cudaStreamEndCapture(b->capture, &gr);
         if (rc) {
             if (gr) cudaGraphDestroy(gr);
             return rc;
@@ -1715,7 +1716,7 @@ extern "C" int lu2gpu_batch_autotune(lu2gpu_batch *b, int *params_out)
                 if (batch_configure(b, cand_threads[ti], cand_pw[pi], cand_ctas[ci])) continue;  // does not fit
                 if ((rc = lu2gpu_batch_restore(b))) return rc;
                 CU_TRY(cudaEventRecord(e0, st));
-                if ((rc = batch_enqueue(b))) return rc;
+                if ((rc = batch_enqueue(b, st))) return rc;
                 CU_TRY(cudaEventRecord(e1, st));
                 CU_TRY(cudaEventSynchronize(e1));
                 float ms = 0;

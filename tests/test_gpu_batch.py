@@ -133,3 +133,20 @@ def test_batch_zero_pivot_reported(ctx):
     info = b.solve()
     assert info[0] == 0 and info[1] == 8
     b.close()
+
+
+def test_batch_on_legacy_default_stream():
+    """A context on the legacy default stream (as torch's current stream is by
+    default): the graph is captured on the batch's own stream and launched there."""
+    c = L.Context(0)
+    c.set_stream(0)
+    n, r = L.batch_sizes(64, 3, 16, 200, 0.2, 4)
+    b = L.Batch(c, n, r)
+    b.generate(9)
+    b.snapshot()
+    for _ in range(2):
+        b.restore()
+        assert (b.solve() == 0).all()
+        assert (b.residuals() < 16).all()
+    b.close()
+    c.close()
