@@ -51,6 +51,10 @@ extern "C" {
 #define LU2GPU_PIVOT_REF 0     /* bug-compatible with lu2tlib.c:1052 (see below) */
 #define LU2GPU_PIVOT_PARTIAL 1 /* true partial pivoting (default) */
 
+/* trailing-update precision of the precision form's factorization */
+#define LU2GPU_UPDATE_BF16 0 /* BF16 operands, per-panel power-of-two scales */
+#define LU2GPU_UPDATE_FP8 1  /* FP8 E4M3 operands, per-128x128-tile power-of-two scales */
+
 /* CBLAS enum values (CBLAS_ORDER / CBLAS_TRANSPOSE) accepted by gdrblas_dgemm */
 #define LU2GPU_CBLAS_ROWMAJOR 101
 #define LU2GPU_CBLAS_COLMAJOR 102
@@ -202,6 +206,33 @@ int lu2gpu_mixed_solve(lu2gpu_ctx *ctx, int n, const double *a, long lda, const 
  * 192, 256}; tcgen05 tensor cores with FP32 accumulation. */
 int lu2gpu_bf16_update_dev(lu2gpu_ctx *ctx, int M, int N, int K, const void *a, long lda, const void *bt, long ldb,
                            float *c, long ldc, float scale);
+
+/* GMRES-IR: A x = b (A FP64 n x n, row stride lda, 16-byte aligned, not
+ * modified) with lu2's factorization of an FP32 copy -- the panel in FP32,
+ * the trailing updates on the tensor cores with FP32 accumulation and `update`
+ * operands: LU2GPU_UPDATE_BF16 (per-panel scales, nb in {64, 128, 192, 256})
+ * or LU2GPU_UPDATE_FP8 (E4M3, per-128x128-tile scales, nb in {128, 256}) --
+ * then iterative refinement whose residual r = b - A x and update of x are in
+ * FP64 and whose correction equations A d = r are solved by GMRES(restart)
+ * (restart <= 32) left-preconditioned by the low-precision factors, with FP64
+ * Arnoldi vectors orthogonalised by classical Gram-Schmidt applied twice.  Each
+ * correction is solved to a preconditioned relative residual of inner_tol.
+ * Stops when the HPL scaled residual is below 16 or after max_iter GMRES
+ * iterations in all.  out (host, may be NULL) receives {refinement steps,
+ * GMRES iterations, final scaled residual, factorization seconds, refinement
+ * seconds}.  Returns 0 when the bound was met, LU2GPU_ERR_NOCONV when not,
+ * > 0 on a zero pivot, < 0 on errors.  No counterpart in the reference. */
+int lu2gpu_gmres_solve(lu2gpu_ctx *ctx, int n, const double *a, long lda, const double *b, double *x, int nb,
+                       int update, int restart, double inner_tol, int max_iter, double *out);
+
+/* The FP8 form's trailing update on its own: a (M x K) and bt (N x K) FP32
+ * device matrices (row strides lda, ldb multiples of 4, 16-byte aligned) are
+ * quantized to E4M3 with one power-of-two scale per 128 x 128 tile, then c
+ * (FP32, M x N, row stride ldc) -= a_q * bt_q^T on the tcgen05 tensor cores
+ * (kind::f8f6f4, FP32 accumulation), K in {128, 256}.  a_deq / bt_deq (device,
+ * may be NULL) receive the dequantized operands (M x K, N x K, contiguous). */
+int lu2gpu_fp8_update_dev(lu2gpu_ctx *ctx, int M, int N, int K, const float *a, long lda, const float *bt, long ldb,
+                          float *c, long ldc, float *a_deq, float *bt_deq);
 
 /* Batching form (no counterpart in the reference, which solves one system
  * per run): many independent systems of uneven order, each lu2's augmented

@@ -8,6 +8,8 @@ from .lu2 import (  # noqa: F401
     CBLAS_TRANS,
     PIVOT_PARTIAL,
     PIVOT_REF,
+    UPDATE_BF16,
+    UPDATE_FP8,
     Batch,
     Context,
     Lu2GpuError,

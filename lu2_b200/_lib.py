@@ -56,6 +56,10 @@ SIGNATURES = {
     "lu2gpu_mixed_solve": (C.c_int, [vp, C.c_int, vp, C.c_long, vp, vp, C.c_int, C.c_int, C.c_int, vp]),
     "lu2gpu_bf16_update_dev": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, vp, C.c_long, vp, C.c_long, vp, C.c_long,
                                          C.c_float]),
+    "lu2gpu_gmres_solve": (C.c_int, [vp, C.c_int, vp, C.c_long, vp, vp, C.c_int, C.c_int, C.c_int, C.c_double,
+                                     C.c_int, vp]),
+    "lu2gpu_fp8_update_dev": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, vp, C.c_long, vp, C.c_long, vp, C.c_long,
+                                        vp, vp]),
     "lu2gpu_batch_create": (C.c_int, [vp, C.c_int, vp, vp, C.POINTER(vp)]),
     "lu2gpu_batch_destroy": (C.c_int, [vp]),
     "lu2gpu_batch_system": (C.c_int, [vp, C.c_int, C.POINTER(vp), C.POINTER(C.c_long)]),

@@ -192,7 +192,7 @@ __global__ void __launch_bounds__(256) residual_kernel(const double *__restrict_
             sa += __shfl_xor_sync(0xffffffffu, sa, o);
         }
         if (lane == 0) {
-            r[i] = b[i] - s;
+            r[i] = b ? b[i] - s : s;  // without b: the product A x
             if (rowabs) rowabs[i] = sa;
         }
     }

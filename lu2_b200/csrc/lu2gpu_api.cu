@@ -1338,6 +1338,17 @@ struct MixedWork {
     unsigned *amax() { return (unsigned *)small; }
     float *scales() { return (float *)((char *)small + 16); }
     unsigned long long *norms() { return (unsigned long long *)((char *)small + 64); }
+    // trailing-update precision of the factorization: BF16 (per-panel scales)
+    // or FP8 E4M3 (per-128x128-tile scales)
+    int update = LU2GPU_UPDATE_BF16;
+    uint8_t *l8 = nullptr, *b8 = nullptr;  // L21 (M x nb) and U12^T (N x nb), E4M3
+    size_t l8_cap = 0, b8_cap = 0;
+    float *dq = nullptr;  // tile dequantization factors of L21 then of U12^T
+    size_t dq_cap = 0;
+    float *bt32top = nullptr;  // U12^T (N x nb) in FP32 from the top-level TRSM
+    size_t bt32top_cap = 0;
+    double *gm = nullptr;  // GMRES: basis (restart+1 vectors), w, z, d, t, partial sums, dots
+    size_t gm_cap = 0;
 };
 
 static void free_mixed(lu2gpu_ctx *c)
@@ -1351,8 +1362,25 @@ static void free_mixed(lu2gpu_ctx *c)
     cudaFree(m->dinv);
     cudaFree(m->vec);
     cudaFree(m->small);
+    cudaFree(m->l8);
+    cudaFree(m->b8);
+    cudaFree(m->dq);
+    cudaFree(m->bt32top);
+    cudaFree(m->gm);
     delete m;
     c->mx = nullptr;
+}
+
+// FP8 form buffers for an n x n matrix with nb-wide panels
+static int fp8_work(lu2gpu_ctx *c, int n, int nb)
+{
+    MixedWork *m = c->mx;
+    int rc;
+    const size_t tiles = ((size_t)n + 127) / 128 + 1;
+    if ((rc = grow((void **)&m->l8, &m->l8_cap, (size_t)n * nb + 1024))) return rc;
+    if ((rc = grow((void **)&m->b8, &m->b8_cap, (size_t)(n + 16) * nb + 1024))) return rc;
+    if ((rc = grow((void **)&m->dq, &m->dq_cap, 2 * tiles * (nb / 128) * sizeof(float) + 256))) return rc;
+    return grow((void **)&m->bt32top, &m->bt32top_cap, (size_t)(n + 16) * nb * sizeof(float) + 1024);
 }
 
 static int mixed_work(lu2gpu_ctx *c, int n, long ld32, int nb)
@@ -1395,6 +1423,24 @@ static int right_part32(lu2gpu_ctx *c, const View32 &v, int k0, int k1, int cs, 
         if (k1 < v.n)
             K_TRY(launch_sgemm_update(v.a + (size_t)k1 * v.ld + k0, v.ld, m->bt32, v.a + (size_t)k1 * v.ld + cs, v.ld,
                                       v.n - k1, ce - cs, K, c->stream));
+        return 0;
+    }
+    if (m->update == LU2GPU_UPDATE_FP8) {
+        const int M = v.n - k1, N = ce - cs;
+        {
+            PhaseTimer t(c, PH_TRSM);
+            // U12 solved in place; its transpose (N x K, FP32) feeds the quantizer
+            K_TRY(launch_trsm_unit_lower_f32(T, v.ld, X, v.ld, K, N, k1 < v.n ? m->bt32top : nullptr, c->stream));
+        }
+        if (k1 < v.n) {
+            PhaseTimer t(c, PH_DGEMM);
+            const float *L = v.a + (size_t)k1 * v.ld + k0;
+            float *dqa = m->dq, *dqb = m->dq + (((size_t)M + 127) / 128) * (K / 128);
+            K_TRY(launch_quant_fp8_tiles(L, v.ld, M, K, m->l8, K, dqa, c->stream));
+            K_TRY(launch_quant_fp8_tiles(m->bt32top, K, N, K, m->b8, K, dqb, c->stream));
+            K_TRY(launch_fp8_update(m->l8, K, dqa, m->b8, K, dqb, v.a + (size_t)k1 * v.ld + cs, v.ld, M, N, K,
+                                    c->d_status, c->stream));
+        }
         return 0;
     }
     {
@@ -1818,6 +1864,7 @@ extern "C" int lu2gpu_mixed_solve(lu2gpu_ctx *c, int n, const double *a, long ld
     int rc = mixed_work(c, n, ld32, nb);
     if (rc) return rc;
     MixedWork *m = c->mx;
+    m->update = LU2GPU_UPDATE_BF16;
     double *r = m->vec + n, *rowabs = m->vec + 2 * (size_t)n;
     float *v32 = reinterpret_cast<float *>(m->vec + 3 * (size_t)n);
     cudaEvent_t ev[3];
@@ -1874,4 +1921,226 @@ extern "C" int lu2gpu_mixed_solve(lu2gpu_ctx *c, int n, const double *a, long ld
         return LU2GPU_ERR_NOCONV;
     }
     return 0;
+}
+
+// ---------------------------------------------------------------------------
+// GMRES-IR
+
+// z = U^{-1} L^{-1} P w with the FP32 factors (FP64 vectors in and out)
+static int precond_apply(lu2gpu_ctx *c, int n, long ld32, int nb, const double *w, double *z)
+{
+    MixedWork *m = c->mx;
+    float *v32 = reinterpret_cast<float *>(m->vec + 3 * (size_t)n);
+    K_TRY(launch_f64_to_f32(w, 1, v32, 1, n, 1, c->stream));
+    int rc = solve32_enqueue(c, n, m->a32, ld32, nb, v32);
+    if (rc) return rc;
+    K_TRY(launch_f32_to_f64(v32, 1, z, 1, n, 1, c->stream));
+    return 0;
+}
+
+extern "C" int lu2gpu_gmres_solve(lu2gpu_ctx *c, int n, const double *a, long lda, const double *b, double *x, int nb,
+                                  int update, int restart, double inner_tol, int max_iter, double *out)
+{
+    if (!c || n <= 0 || !a || !b || !x || lda < n || restart < 1 || restart > 32 || max_iter < 1 ||
+        !(inner_tol > 0.0 && inner_tol < 1.0)) {
+        set_error("lu2gpu_gmres_solve: bad arguments (restart in [1, 32], max_iter >= 1, 0 < inner_tol < 1)");
+        return LU2GPU_ERR_ARG;
+    }
+    if ((lda & 1) || (reinterpret_cast<uintptr_t>(a) & 15)) {
+        set_error("lu2gpu_gmres_solve: A must be 16-byte aligned with an even row stride");
+        return LU2GPU_ERR_ARG;
+    }
+    if (update == LU2GPU_UPDATE_BF16) {
+        if (nb < 64 || nb > 256 || (nb % 64)) {
+            set_error("lu2gpu_gmres_solve: nb=%d must be 64, 128, 192 or 256 for the BF16 update", nb);
+            return LU2GPU_ERR_ARG;
+        }
+    } else if (update == LU2GPU_UPDATE_FP8) {
+        if (nb != 128 && nb != 256) {
+            set_error("lu2gpu_gmres_solve: nb=%d must be 128 or 256 for the FP8 update", nb);
+            return LU2GPU_ERR_ARG;
+        }
+    } else {
+        set_error("lu2gpu_gmres_solve: unknown update precision %d", update);
+        return LU2GPU_ERR_ARG;
+    }
+    DeviceGuard g(c->device);
+    const long ld32 = ((long)n + 31) & ~31L;
+    int rc = mixed_work(c, n, ld32, nb);
+    if (rc) return rc;
+    MixedWork *m = c->mx;
+    m->update = update;
+    if (update == LU2GPU_UPDATE_FP8 && (rc = fp8_work(c, n, nb))) return rc;
+    const long ldv = ((long)n + 31) & ~31L;
+    const size_t gm_doubles = (size_t)(restart + 1 + 4) * ldv + 64 * MULTI_DOT_BLOCKS + 256;
+    if ((rc = grow((void **)&m->gm, &m->gm_cap, gm_doubles * sizeof(double)))) return rc;
+    double *V = m->gm, *w = V + (size_t)(restart + 1) * ldv, *z = w + ldv, *d = z + ldv, *t = d + ldv;
+    double *partial = t + ldv, *dots = partial + 64 * MULTI_DOT_BLOCKS;  // dots: h[32] h2[32] |z|^2 . y[32] one
+    double *r = m->vec + n, *rowabs = m->vec + 2 * (size_t)n;
+    cudaEvent_t ev[3];
+    for (int i = 0; i < 3; i++) CU_TRY(cudaEventCreate(&ev[i]));
+    if ((rc = begin_status(c))) return rc;
+    CU_TRY(cudaEventRecord(ev[0], c->stream));
+    K_TRY(launch_f64_to_f32(a, lda, m->a32, ld32, n, n, c->stream));
+    if ((rc = factor32_or_fail(c, n, m->a32, ld32, nb, LU2GPU_PIVOT_PARTIAL))) return rc;
+    CU_TRY(cudaEventRecord(ev[1], c->stream));
+
+    const double one = 1.0;
+    CU_TRY(cudaMemcpyAsync(dots + 128, &one, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CU_TRY(cudaMemsetAsync(x, 0, (size_t)n * sizeof(double), c->stream));
+    K_TRY(launch_residual(a, lda, n, b, x, r, rowabs, c->stream));  // r = b, row sums of |A|
+    CU_TRY(cudaMemsetAsync(m->norms(), 0, 4 * sizeof(unsigned long long), c->stream));
+    K_TRY(launch_vec_absmax(b, n, m->norms() + 2, c->stream));
+    K_TRY(launch_vec_absmax(rowabs, n, m->norms() + 3, c->stream));
+    const double eps = 1.1102230246251565e-16;  // 2^-53
+    double bnorm = 0, anorm = 0;
+    auto hpl_now = [&](double *h) -> int {
+        CU_TRY(cudaMemsetAsync(m->norms(), 0, 2 * sizeof(unsigned long long), c->stream));
+        K_TRY(launch_vec_absmax(r, n, m->norms(), c->stream));
+        K_TRY(launch_vec_absmax(x, n, m->norms() + 1, c->stream));
+        unsigned long long nb_h[4];
+        CU_TRY(cudaMemcpyAsync(nb_h, m->norms(), 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+        CU_TRY(cudaStreamSynchronize(c->stream));
+        double v[4];
+        memcpy(v, nb_h, sizeof(v));
+        bnorm = v[2];
+        anorm = v[3];
+        *h = v[0] / (eps * (anorm * v[1] + bnorm) * n);
+        return 0;
+    };
+    // |z| on the host (one dot product)
+    auto norm_of = [&](const double *vec, double *nrm) -> int {
+        K_TRY(launch_multi_dot(vec, ldv, 1, vec, n, partial, dots + 64, c->stream));
+        double s = 0;
+        CU_TRY(cudaMemcpyAsync(&s, dots + 64, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CU_TRY(cudaStreamSynchronize(c->stream));
+        *nrm = sqrt(s);
+        return 0;
+    };
+
+    double H[33][32], cs[32], sn[32], gvec[33], hpl = 0;
+    int total = 0, outer = 0;
+    for (;;) {
+        if ((rc = hpl_now(&hpl))) return rc;
+        if (hpl < 16.0 || total >= max_iter) break;
+        outer++;
+        // correction equation A d = r, left-preconditioned: M^{-1} A d = M^{-1} r
+        CU_TRY(cudaMemsetAsync(d, 0, (size_t)n * sizeof(double), c->stream));
+        if ((rc = precond_apply(c, n, ld32, nb, r, z))) return rc;
+        double beta0 = 0;
+        if ((rc = norm_of(z, &beta0))) return rc;
+        if (!(beta0 > 0.0)) break;  // r = 0
+        double beta = beta0;
+        bool conv = false;
+        while (!conv && total < max_iter) {
+            K_TRY(launch_vec_scale(z, 1.0 / beta, V, n, c->stream));
+            for (int i = 0; i <= restart; i++) gvec[i] = 0.0;
+            gvec[0] = beta;
+            int k = 0;
+            while (k < restart && total < max_iter) {
+                double *vk = V + (size_t)k * ldv;
+                K_TRY(launch_residual(a, lda, n, nullptr, vk, w, nullptr, c->stream));  // w = A v_k
+                if ((rc = precond_apply(c, n, ld32, nb, w, z))) return rc;
+                // classical Gram-Schmidt, twice
+                K_TRY(launch_multi_dot(V, ldv, k + 1, z, n, partial, dots, c->stream));
+                K_TRY(launch_multi_axpy(V, ldv, k + 1, dots, -1.0, z, n, c->stream));
+                K_TRY(launch_multi_dot(V, ldv, k + 1, z, n, partial, dots + 32, c->stream));
+                K_TRY(launch_multi_axpy(V, ldv, k + 1, dots + 32, -1.0, z, n, c->stream));
+                K_TRY(launch_multi_dot(z, ldv, 1, z, n, partial, dots + 64, c->stream));
+                double hd[65];
+                CU_TRY(cudaMemcpyAsync(hd, dots, 65 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+                CU_TRY(cudaStreamSynchronize(c->stream));
+                total++;
+                for (int j = 0; j <= k; j++) H[j][k] = hd[j] + hd[32 + j];
+                const double hk1 = sqrt(hd[64] > 0 ? hd[64] : 0.0);
+                // previous rotations, then the one that zeroes H[k+1][k]
+                for (int j = 0; j < k; j++) {
+                    const double t0 = cs[j] * H[j][k] + sn[j] * H[j + 1][k];
+                    H[j + 1][k] = -sn[j] * H[j][k] + cs[j] * H[j + 1][k];
+                    H[j][k] = t0;
+                }
+                const double den = hypot(H[k][k], hk1);
+                cs[k] = den > 0 ? H[k][k] / den : 1.0;
+                sn[k] = den > 0 ? hk1 / den : 0.0;
+                H[k][k] = den;
+                gvec[k + 1] = -sn[k] * gvec[k];
+                gvec[k] = cs[k] * gvec[k];
+                k++;
+                if (fabs(gvec[k]) <= inner_tol * beta0 || !(hk1 > 0.0)) {
+                    conv = true;
+                    break;
+                }
+                if (k < restart) K_TRY(launch_vec_scale(z, 1.0 / hk1, V + (size_t)k * ldv, n, c->stream));
+            }
+            // y = H(0:k, 0:k)^{-1} g(0:k); d += V y
+            double y[32];
+            for (int i = k - 1; i >= 0; i--) {
+                double s = gvec[i];
+                for (int j = i + 1; j < k; j++) s -= H[i][j] * y[j];
+                y[i] = H[i][i] != 0.0 ? s / H[i][i] : 0.0;
+            }
+            if (k > 0) {
+                CU_TRY(cudaMemcpy(dots + 96, y, (size_t)k * sizeof(double), cudaMemcpyHostToDevice));
+                K_TRY(launch_multi_axpy(V, ldv, k, dots + 96, 1.0, d, n, c->stream));
+            }
+            if (!conv && total < max_iter) {
+                // restart from the true correction residual r - A d
+                K_TRY(launch_residual(a, lda, n, r, d, t, nullptr, c->stream));
+                if ((rc = precond_apply(c, n, ld32, nb, t, z))) return rc;
+                if ((rc = norm_of(z, &beta))) return rc;
+                if (!(beta > inner_tol * beta0)) conv = true;
+            }
+        }
+        K_TRY(launch_multi_axpy(d, ldv, 1, dots + 128, 1.0, x, n, c->stream));  // x += d
+        K_TRY(launch_residual(a, lda, n, b, x, r, nullptr, c->stream));         // r = b - A x
+    }
+    CU_TRY(cudaEventRecord(ev[2], c->stream));
+    rc = end_status(c, "lu2gpu_gmres_solve");
+    float t_fac = 0, t_ir = 0;
+    cudaEventElapsedTime(&t_fac, ev[0], ev[1]);
+    cudaEventElapsedTime(&t_ir, ev[1], ev[2]);
+    for (int i = 0; i < 3; i++) cudaEventDestroy(ev[i]);
+    if (out) {
+        out[0] = outer;
+        out[1] = total;
+        out[2] = hpl;
+        out[3] = t_fac * 1e-3;
+        out[4] = t_ir * 1e-3;
+    }
+    if (rc) return rc;
+    if (!(hpl < 16.0)) {
+        set_error("lu2gpu_gmres_solve: scaled residual %.3g after %d GMRES iterations (%d refinement steps)", hpl,
+                  total, outer);
+        return LU2GPU_ERR_NOCONV;
+    }
+    return 0;
+}
+
+extern "C" int lu2gpu_fp8_update_dev(lu2gpu_ctx *c, int M, int N, int K, const float *a, long lda, const float *bt,
+                                     long ldb, float *c32, long ldc, float *a_deq, float *bt_deq)
+{
+    if (!c || M < 0 || N < 0 || (K != 128 && K != 256) || !a || !bt || !c32 || lda < K || ldb < K || (lda & 3) ||
+        (ldb & 3) || (reinterpret_cast<uintptr_t>(a) & 15) || (reinterpret_cast<uintptr_t>(bt) & 15)) {
+        set_error("lu2gpu_fp8_update_dev: bad arguments (K must be 128 or 256, strides multiples of 4, "
+                  "16-byte aligned operands)");
+        return LU2GPU_ERR_ARG;
+    }
+    if (M == 0 || N == 0) return 0;
+    DeviceGuard g(c->device);
+    int rc = ensure_work(c, 16, 16, 16);
+    if (rc) return rc;
+    double *s0, *s1, *s2;
+    const size_t tm = ((size_t)M + 127) / 128, tn = ((size_t)N + 127) / 128;
+    if ((rc = stage(c, 0, ((size_t)M * K + 7) / 8, &s0)) || (rc = stage(c, 1, ((size_t)N * K + 7) / 8, &s1)) ||
+        (rc = stage(c, 2, (tm + tn) * (K / 128), &s2)))
+        return rc;
+    uint8_t *a8 = reinterpret_cast<uint8_t *>(s0), *b8 = reinterpret_cast<uint8_t *>(s1);
+    float *dqa = reinterpret_cast<float *>(s2), *dqb = dqa + tm * (K / 128);
+    if ((rc = begin_status(c))) return rc;
+    K_TRY(launch_quant_fp8_tiles(a, lda, M, K, a8, K, dqa, c->stream));
+    K_TRY(launch_quant_fp8_tiles(bt, ldb, N, K, b8, K, dqb, c->stream));
+    if (a_deq) K_TRY(launch_dequant_fp8_tiles(a8, K, dqa, M, K, a_deq, K, c->stream));
+    if (bt_deq) K_TRY(launch_dequant_fp8_tiles(b8, K, dqb, N, K, bt_deq, K, c->stream));
+    K_TRY(launch_fp8_update(a8, K, dqa, b8, K, dqb, c32, ldc, M, N, K, c->d_status, c->stream));
+    return end_status(c, "lu2gpu_fp8_update_dev");
 }

@@ -163,8 +163,8 @@ cudaError_t launch_panel_scales(const unsigned *amax_bits, float *scales, cudaSt
 // y = FP32(x) for an n x cols FP64 block and back
 cudaError_t launch_f64_to_f32(const double *x, long ldx, float *y, long ldy, int rows, int cols, cudaStream_t st);
 cudaError_t launch_f32_to_f64(const float *x, long ldx, double *y, long ldy, int rows, int cols, cudaStream_t st);
-// r = b - A x (FP64, A n x n stride lda, b and x n-vectors); rowsum (optional)
-// receives sum_j |a_ij| for the HPL norm
+// r = b - A x (FP64, A n x n stride lda, b and x n-vectors), or r = A x when b
+// is null; rowabs (optional) receives sum_j |a_ij| for the HPL norm
 cudaError_t launch_residual(const double *a, long lda, int n, const double *b, const double *x, double *r,
                             double *rowabs, cudaStream_t st);
 // per-panel update of the forward solve: y[rows] -= L (rows x K, stride ld) * v (K)
@@ -200,6 +200,26 @@ cudaError_t launch_batch_generate(double *data, const BatchSys *sys, int count, 
                                   cudaStream_t st);
 // *out = max(*out, max |v|) as double bits
 cudaError_t launch_vec_absmax(const double *v, int n, unsigned long long *out, cudaStream_t st);
+
+// FP8 form (kernels_fp8.cu): C (FP32) -= sum_kb da(tile_m,kb) db(tile_n,kb) Aq_kb Bq_kb^T with
+// E4M3 operands a8 (M x K, row stride lda bytes) and bt8 (N x K), K = 128 or 256
+cudaError_t launch_fp8_update(const uint8_t *a8, long lda, const float *da, const uint8_t *bt8, long ldb,
+                              const float *db, float *c, long ldc, int M, int N, int K, int *status, cudaStream_t st);
+// per-128x128-tile E4M3 quantization with power-of-two scales; dq = [ceil(rows/128)][cols/128]
+cudaError_t launch_quant_fp8_tiles(const float *x, long ldx, int rows, int cols, uint8_t *q, long ldq, float *dq,
+                                   cudaStream_t st);
+cudaError_t launch_dequant_fp8_tiles(const uint8_t *q, long ldq, const float *dq, int rows, int cols, float *y,
+                                     long ldy, cudaStream_t st);
+
+// GMRES vector kernels (kernels_gmres.cu)
+constexpr int MULTI_DOT_BLOCKS = 148;
+// out[j] = <V[j], z>, j < k; partial: k * MULTI_DOT_BLOCKS doubles
+cudaError_t launch_multi_dot(const double *V, long ldv, int k, const double *z, int n, double *partial, double *out,
+                             cudaStream_t st);
+// z += sign * sum_{j<k} c[j] V[j] (k <= 64, c on the device)
+cudaError_t launch_multi_axpy(const double *V, long ldv, int k, const double *c, double sign, double *z, int n,
+                              cudaStream_t st);
+cudaError_t launch_vec_scale(const double *x, double alpha, double *y, int n, cudaStream_t st);
 
 // lu2's matrix generator (randomsetmat, lu2.c:70-85) on the device, bit-identical to
 // glibc drand48: row i holds draws i*(n+1) .. i*(n+1)+n (b_i last); extra

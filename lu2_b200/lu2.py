@@ -19,6 +19,8 @@ from . import _lib
 
 PIVOT_REF = 0
 PIVOT_PARTIAL = 1
+UPDATE_BF16 = 0
+UPDATE_FP8 = 1
 CBLAS_ROWMAJOR, CBLAS_COLMAJOR, CBLAS_NOTRANS, CBLAS_TRANS = 101, 102, 111, 112
 TIMER_NAMES = ["col dec t", "swaprows", "solve tri", "DGEMMrest", "backward_sub", "panel update"]
 
@@ -172,6 +174,26 @@ class Context:
         if rc < 0 and rc != -6:
             raise Lu2GpuError("lu2gpu_mixed_solve", rc)
         return res
+
+    def gmres_solve(self, a, n: int, lda: int, b, x, nb: int = 256, update: int = UPDATE_FP8, restart: int = 30,
+                    inner_tol: float = 1e-6, max_iter: int = 300) -> dict:
+        """GMRES-IR: FP32 panel + BF16/FP8 trailing updates, FP64 refinement with
+        GMRES(restart) on the correction equations (device a, b, x)."""
+        out = np.zeros(5, dtype=np.float64)
+        rc = lib().lu2gpu_gmres_solve(self._h, n, _ptr(a), lda, _ptr(b), _ptr(x), nb, update, restart, inner_tol,
+                                      max_iter, _ptr(out))
+        res = {"status": rc, "refinements": int(out[0]), "gmres_iterations": int(out[1]), "hpl": float(out[2]),
+               "factor_s": float(out[3]), "refine_s": float(out[4])}
+        if rc < 0 and rc != -6:
+            raise Lu2GpuError("lu2gpu_gmres_solve", rc)
+        return res
+
+    def fp8_update(self, M, N, K, a32, lda, bt32, ldb, c32, ldc, a_deq=None, bt_deq=None) -> None:
+        """c -= q(a) q(bt)^T with per-128x128-tile E4M3 quantization (FP32 device arrays)."""
+        _check("lu2gpu_fp8_update_dev",
+               lib().lu2gpu_fp8_update_dev(self._h, M, N, K, _ptr(a32), lda, _ptr(bt32), ldb, _ptr(c32), ldc,
+                                           _ptr(a_deq) if a_deq is not None else None,
+                                           _ptr(bt_deq) if bt_deq is not None else None))
 
     def bf16_update(self, M, N, K, a16, lda, bt16, ldb, c32, ldc, scale=1.0) -> None:
         _check("lu2gpu_bf16_update_dev", lib().lu2gpu_bf16_update_dev(self._h, M, N, K, _ptr(a16), lda, _ptr(bt16),
