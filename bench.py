@@ -302,6 +302,110 @@ def run_batched(ctx, dev, stream, args, max_over_ranks, world) -> dict:
             "speedup_vs_loop": sps / (world / t_loop)}
 
 
+def fp8_update_bytes(n: int, nb: int) -> float:
+    """Algorithmic HBM bytes of the FP8 trailing updates of an order-n factorization:
+    FP32 C read and written (8 B per element) plus the E4M3 operands (1 B each)."""
+    tot = 0.0
+    for i in range(0, n, nb):
+        w = min(nb, n - i)
+        m = n - i - w
+        tot += 8.0 * m * m + 1.0 * w * 2 * m
+    return tot
+
+
+def run_fp8(ctx, dev, stream, args, max_over_ranks, world) -> dict:
+    """FP8 form: lu2's factorization of an FP32 copy with E4M3 trailing updates
+    (per-128x128-tile power-of-two scales, FP32 accumulation), then GMRES-IR
+    (restart 30) in FP64.  Forward error against the plain FP64 GPU solve at
+    N = args.fp8_check_n (general and diagonally dominant matrices); timed solve
+    of the diagonally dominant matrix at N = args.fp8_n; the general matrix at
+    N = args.fp8_n with a bounded GMRES iteration budget."""
+    import torch
+
+    import lu2_b200 as L
+
+    out = {"update": "FP8 E4M3 operands, per-128x128-tile power-of-two scales, FP32 accumulation (tcgen05 "
+                     "kind::f8f6f4); FP32 panel; GMRES(30)-IR in FP64 preconditioned by the FP32/FP8 factors",
+           "nb": args.fp8_nb}
+    nb = args.fp8_nb
+
+    def system(n, kind):
+        ld = L.device_ld(n)
+        a = torch.empty((n, ld), dtype=torch.float64, device=dev)
+        ctx.generate(a, n, ld, 1, 1, kind=kind)
+        return a, ld, a[:, n].clone()
+
+    # forward error against the plain FP64 solve of the same system
+    nc = args.fp8_check_n
+    checks = {}
+    for kind, name in ((0, "general"), (1, "diagonally_dominant")):
+        a, ld, b = system(nc, kind)
+        a64 = a.clone()
+        if ctx.lusolve(a64, nc, ld, 256, 1, L.PIVOT_PARTIAL) != 0:
+            raise RuntimeError("FP64 reference solve hit a zero pivot")
+        x64 = a64[:, nc].clone()
+        del a64
+        x = torch.zeros(nc, dtype=torch.float64, device=dev)
+        res = ctx.gmres_solve(a, nc, ld, b, x, nb, update=L.UPDATE_FP8, restart=30,
+                              max_iter=args.fp8_general_iters)
+        res["fwd_err_vs_fp64"] = ((x - x64).abs().max() / x64.abs().max()).item()
+        res["converged"] = res.pop("status") == 0
+        checks[name] = res
+        del a, b, x, x64
+        torch.cuda.empty_cache()
+    out["check_n%d" % nc] = checks
+
+    n = args.fp8_n
+    a, ld, b = system(n, 1)
+    x = torch.zeros(n, dtype=torch.float64, device=dev)
+    for _ in range(args.fp8_warmup):
+        ctx.gmres_solve(a, n, ld, b, x, nb, update=L.UPDATE_FP8, restart=30, max_iter=100)
+    torch.cuda.synchronize()
+    ts, res = [], None
+    for _ in range(args.fp8_steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        res = ctx.gmres_solve(a, n, ld, b, x, nb, update=L.UPDATE_FP8, restart=30, max_iter=100)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1) / 1e3)
+    t = max_over_ranks(sum(ts) / len(ts))
+    ctx.set_timing(True)
+    ctx.gmres_solve(a, n, ld, b, x, nb, update=L.UPDATE_FP8, restart=30, max_iter=100)
+    timers = ctx.timers()
+    ctx.set_timing(False)
+    upd_ms = timers["DGEMMrest"][0]
+    upd_bytes = fp8_update_bytes(n, nb)
+    out["diagonally_dominant_n%d" % n] = {
+        "metric": "FP64-equivalent GFLOP/s (2/3 N^3 + 2 N^2)/t", "value": world * lu_flops(n) / t / 1e9,
+        "seconds": t, "steps": len(ts), "warmup": args.fp8_warmup, "converged": res["status"] == 0,
+        "refinements": res["refinements"], "gmres_iterations": res["gmres_iterations"], "hpl_residual": res["hpl"],
+        "factor_s": res["factor_s"], "refine_s": res["refine_s"],
+        "fp8_update": {"ms": upd_ms, "launches": timers["DGEMMrest"][1], "algorithmic_bytes": upd_bytes,
+                       "hbm_gbs": upd_bytes / (upd_ms / 1e3) / 1e9 if upd_ms > 0 else None},
+        "phases_ms": {k: {"ms": v[0], "launches": v[1]} for k, v in timers.items()}}
+    del a, b, x
+    torch.cuda.empty_cache()
+
+    a, ld, b = system(n, 0)
+    x = torch.zeros(n, dtype=torch.float64, device=dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    res = ctx.gmres_solve(a, n, ld, b, x, nb, update=L.UPDATE_FP8, restart=30, max_iter=args.fp8_general_iters)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    out["general_n%d" % n] = {"converged": res["status"] == 0, "hpl_residual": res["hpl"],
+                              "gmres_iterations": res["gmres_iterations"], "iteration_budget": args.fp8_general_iters,
+                              "refinements": res["refinements"], "finite_factors": res["finite_factors"],
+                              "factor_s": res["factor_s"],
+                              "refine_s": res["refine_s"], "seconds": e0.elapsed_time(e1) / 1e3}
+    del a, b, x
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_reference(args, rank: int) -> None:
     if rank != 0:
         return
@@ -354,6 +458,16 @@ def main() -> int:
                     help="profiling run for ncu: generate the matrix and run exactly one factor+solve step")
     ap.add_argument("--profile-mixed", action="store_true",
                     help="profiling run for ncu: one BF16-LU + IR solve of the diagonally dominant system")
+    ap.add_argument("--profile-fp8", action="store_true",
+                    help="profiling run for ncu: one FP8-LU + GMRES-IR solve of the diagonally dominant system")
+    ap.add_argument("--no-fp8", action="store_true", help="skip the FP8 + GMRES-IR measurement")
+    ap.add_argument("--fp8-n", type=int, default=98304)
+    ap.add_argument("--fp8-nb", type=int, default=256)
+    ap.add_argument("--fp8-check-n", type=int, default=32768)
+    ap.add_argument("--fp8-warmup", type=int, default=1)
+    ap.add_argument("--fp8-steps", type=int, default=1)
+    ap.add_argument("--fp8-general-iters", type=int, default=60,
+                    help="GMRES iteration budget for the general (not diagonally dominant) matrices")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -405,13 +519,16 @@ def main() -> int:
         if info != 0:
             raise RuntimeError("zero pivot at column %d" % (info - 1))
 
-    if args.profile_mixed:
+    if args.profile_mixed or args.profile_fp8:
         ctx.generate(pristine, n, ld, 1, 1, kind=1)
         b = pristine[:, n].clone()
         x = torch.zeros(n, dtype=torch.float64, device=dev)
-        res = ctx.mixed_solve(pristine, n, ld, b, x, args.mixed_nb)
+        if args.profile_fp8:
+            res = ctx.gmres_solve(pristine, n, ld, b, x, args.fp8_nb, update=L.UPDATE_FP8, restart=30, max_iter=100)
+        else:
+            res = ctx.mixed_solve(pristine, n, ld, b, x, args.mixed_nb)
         torch.cuda.synchronize()
-        print(json.dumps({"profile_mixed": res, "n": n}))
+        print(json.dumps({"profile_fp8" if args.profile_fp8 else "profile_mixed": res, "n": n}))
         ctx.close()
         return 0
     if args.profile:
@@ -514,10 +631,13 @@ def main() -> int:
         torch.cuda.empty_cache()
         forms["bf16_ir"] = run_mixed(ctx, n, nb, ld, pristine, dev, stream, args, barrier, max_over_ranks,
                                      t / args.steps, world)
-    if not args.no_batched:
+    if "pristine" in locals():
         del pristine
-        torch.cuda.empty_cache()
+    torch.cuda.empty_cache()
+    if not args.no_batched:
         forms["batched_fp64"] = run_batched(ctx, dev, stream, args, max_over_ranks, world)
+    if not args.no_fp8:
+        forms["fp8_gmres_ir"] = run_fp8(ctx, dev, stream, args, max_over_ranks, world)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -220,7 +220,7 @@ int lu2gpu_bf16_update_dev(lu2gpu_ctx *ctx, int M, int N, int K, const void *a, 
  * Stops when the HPL scaled residual is below 16 or after max_iter GMRES
  * iterations in all.  out (host, may be NULL) receives {refinement steps,
  * GMRES iterations, final scaled residual, factorization seconds, refinement
- * seconds}.  Returns 0 when the bound was met, LU2GPU_ERR_NOCONV when not,
+ * seconds, 1 if the preconditioner stayed finite else 0}.  Returns 0 when the bound was met, LU2GPU_ERR_NOCONV when not,
  * > 0 on a zero pivot, < 0 on errors.  No counterpart in the reference. */
 int lu2gpu_gmres_solve(lu2gpu_ctx *ctx, int n, const double *a, long lda, const double *b, double *x, int nb,
                        int update, int restart, double inner_tol, int max_iter, double *out);

@@ -2020,6 +2020,7 @@ extern "C" int lu2gpu_gmres_solve(lu2gpu_ctx *c, int n, const double *a, long ld
 
     double H[33][32], cs[32], sn[32], gvec[33], hpl = 0;
     int total = 0, outer = 0;
+    bool finite = true;  // the preconditioner maps finite vectors to finite vectors
     for (;;) {
         if ((rc = hpl_now(&hpl))) return rc;
         if (hpl < 16.0 || total >= max_iter) break;
@@ -2029,6 +2030,10 @@ extern "C" int lu2gpu_gmres_solve(lu2gpu_ctx *c, int n, const double *a, long ld
         if ((rc = precond_apply(c, n, ld32, nb, r, z))) return rc;
         double beta0 = 0;
         if ((rc = norm_of(z, &beta0))) return rc;
+        if (!std::isfinite(beta0)) {  // the low-precision factors overflowed
+            finite = false;
+            break;
+        }
         if (!(beta0 > 0.0)) break;  // r = 0
         double beta = beta0;
         bool conv = false;
@@ -2106,8 +2111,14 @@ extern "C" int lu2gpu_gmres_solve(lu2gpu_ctx *c, int n, const double *a, long ld
         out[2] = hpl;
         out[3] = t_fac * 1e-3;
         out[4] = t_ir * 1e-3;
+        out[5] = finite ? 1.0 : 0.0;
     }
     if (rc) return rc;
+    if (!finite) {
+        set_error("lu2gpu_gmres_solve: the low-precision factors are not finite (element growth in the "
+                  "factorization); no refinement possible");
+        return LU2GPU_ERR_NOCONV;
+    }
     if (!(hpl < 16.0)) {
         set_error("lu2gpu_gmres_solve: scaled residual %.3g after %d GMRES iterations (%d refinement steps)", hpl,
                   total, outer);

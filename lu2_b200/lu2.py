@@ -179,11 +179,11 @@ class Context:
                     inner_tol: float = 1e-6, max_iter: int = 300) -> dict:
         """GMRES-IR: FP32 panel + BF16/FP8 trailing updates, FP64 refinement with
         GMRES(restart) on the correction equations (device a, b, x)."""
-        out = np.zeros(5, dtype=np.float64)
+        out = np.zeros(6, dtype=np.float64)
         rc = lib().lu2gpu_gmres_solve(self._h, n, _ptr(a), lda, _ptr(b), _ptr(x), nb, update, restart, inner_tol,
                                       max_iter, _ptr(out))
         res = {"status": rc, "refinements": int(out[0]), "gmres_iterations": int(out[1]), "hpl": float(out[2]),
-               "factor_s": float(out[3]), "refine_s": float(out[4])}
+               "factor_s": float(out[3]), "refine_s": float(out[4]), "finite_factors": bool(out[5])}
         if rc < 0 and rc != -6:
             raise Lu2GpuError("lu2gpu_gmres_solve", rc)
         return res
