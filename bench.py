@@ -261,24 +261,37 @@ def run_batched(ctx, dev, stream, args, max_over_ranks, world) -> dict:
     b = L.Batch(ctx, n, r)
     b.generate(1)
     b.snapshot()
-    cfg = b.autotune()
-    for _ in range(args.warmup):
-        b.restore()
-        b.solve()
-    ts = []
-    for _ in range(args.steps):
-        b.restore()
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        info = b.solve()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        ts.append(e0.elapsed_time(e1) / 1e3)
-    t = max_over_ranks(sum(ts) / len(ts))
-    res = b.residuals()
     flops = float(np.sum(2.0 / 3.0 * n.astype(np.float64) ** 3 + 2.0 * n.astype(np.float64) ** 2 * r))
+
+    def timed():
+        """autotune, warm up, time args.steps solves (inputs restored untimed)"""
+        cfg = b.autotune()
+        for _ in range(args.warmup):
+            b.restore()
+            b.solve()
+        ts = []
+        for _ in range(args.steps):
+            b.restore()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            info = b.solve()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1) / 1e3)
+        return cfg, max_over_ranks(sum(ts) / len(ts)), info, b.residuals(), len(ts)
+
+    # FP32 factors + FP64 refinement first, then the plain FP64 variant
+    b.set_mode(L.BATCH_FP32_IR, 10)
+    cfg_ir, t_ir, info_ir, res_ir, _ = timed()
+    its = b.iterations()
+    fp32_ir = {"value": world * count / t_ir, "unit": "systems/s", "seconds": t_ir,
+               "fp64_equivalent_gflops": world * flops / t_ir / 1e9, "max_hpl_residual": float(res_ir.max()),
+               "all_below_16": bool((res_ir < 16).all()), "zero_pivots": int((info_ir != 0).sum()),
+               "refinement_iterations": {"mean": float(its.mean()), "max": int(its.max())}, "autotuned": cfg_ir}
+    b.set_mode(L.BATCH_FP64)
+    cfg, t, info, res, nsteps = timed()
     # the loop of single plain-method launches, on a sample of systems
     rng = np.random.default_rng(0)
     sample = rng.choice(count, size=min(args.batch_loop_sample, count), replace=False)
@@ -296,10 +309,10 @@ def run_batched(ctx, dev, stream, args, max_over_ranks, world) -> dict:
             "gflops": world * flops / t / 1e9, "flops": flops,
             "sizes": "N log-uniform in [16, 512] (seed 1), 10% with 8 right-hand sides, entries lu2 stream seed 1+i",
             "max_hpl_residual": float(res.max()), "all_below_16": bool((res < 16).all()),
-            "zero_pivots": int((info != 0).sum()), "autotuned": cfg, "steps": len(ts), "warmup": args.warmup,
+            "zero_pivots": int((info != 0).sum()), "autotuned": cfg, "steps": nsteps, "warmup": args.warmup,
             "loop_baseline": {"solves_per_s": 1.0 / t_loop, "sample_systems": int(len(sample)),
                               "api": "lu2gpu_lusolve per system (nb=64), host-timed loop"},
-            "speedup_vs_loop": sps / (world / t_loop)}
+            "speedup_vs_loop": sps / (world / t_loop), "fp32_lu_fp64_ir": fp32_ir}
 
 
 def fp8_update_bytes(n: int, nb: int) -> float:

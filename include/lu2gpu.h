@@ -250,6 +250,18 @@ int lu2gpu_batch_generate(lu2gpu_batch *b, long seed);
 /* Keep a copy of the current systems (for residuals and for re-running). */
 int lu2gpu_batch_snapshot(lu2gpu_batch *b);
 int lu2gpu_batch_restore(lu2gpu_batch *b);
+/* Arithmetic of lu2gpu_batch_solve: LU2GPU_BATCH_FP64 (default) factors and
+ * solves in FP64; LU2GPU_BATCH_FP32_IR factors an FP32 copy of each system
+ * (full-width row exchanges, lu2's 1/pivot row scaling) and refines x in
+ * FP64 -- r = b - A x from the unchanged FP64 system, corrections from the
+ * FP32 factors -- until every right-hand side's HPL scaled residual is below
+ * 16 or max_iter corrections were applied (systems with at most 8 right-hand
+ * sides).  Resets the launch shape to the mode's default. */
+#define LU2GPU_BATCH_FP64 0
+#define LU2GPU_BATCH_FP32_IR 1
+int lu2gpu_batch_set_mode(lu2gpu_batch *b, int mode, int max_iter);
+/* Corrections each system took in the last FP32_IR solve (count ints). */
+int lu2gpu_batch_iterations(lu2gpu_batch *b, int *iters_host);
 /* Launch shape: threads per CTA, panel width of the blocked path, CTAs per SM. */
 int lu2gpu_batch_set_config(lu2gpu_batch *b, int threads, int pw, int ctas_per_sm);
 /* Time the launch shapes on this batch and keep the fastest; params_out (4

@@ -10,6 +10,8 @@ from .lu2 import (  # noqa: F401
     PIVOT_REF,
     UPDATE_BF16,
     UPDATE_FP8,
+    BATCH_FP64,
+    BATCH_FP32_IR,
     Batch,
     Context,
     Lu2GpuError,

@@ -67,6 +67,8 @@ SIGNATURES = {
     "lu2gpu_batch_snapshot": (C.c_int, [vp]),
     "lu2gpu_batch_restore": (C.c_int, [vp]),
     "lu2gpu_batch_set_config": (C.c_int, [vp, C.c_int, C.c_int, C.c_int]),
+    "lu2gpu_batch_set_mode": (C.c_int, [vp, C.c_int, C.c_int]),
+    "lu2gpu_batch_iterations": (C.c_int, [vp, vp]),
     "lu2gpu_batch_autotune": (C.c_int, [vp, vp]),
     "lu2gpu_batch_solve": (C.c_int, [vp, vp]),
     "lu2gpu_batch_residuals": (C.c_int, [vp, vp]),

@@ -1,0 +1,465 @@
+// kernels_batch_ir.cu -- the batching form's FP32-LU + FP64 iterative
+// refinement variant: every system's FP64 augmented matrix (left unchanged
+// until x is written into its b columns) is converted to FP32, factored in
+// FP32, and refined in FP64 -- r = b - A x from the FP64 matrix, the
+// correction solved with the FP32 factors -- until every right-hand side has
+// an HPL scaled residual below 16 (or max_iter corrections).
+//
+// Factor storage follows lu2's elimination (lu2.c:541-554, lu2tlib.c:1057-
+// 1059): the pivot row is scaled by 1/pivot right of the diagonal (a unit
+// upper U'), the columns below keep the unscaled multipliers times the pivot
+// (L' lower with the pivots on its diagonal).  Unlike lu2, whose solve rides
+// along as augmented columns, the refinement needs the factors for new
+// right-hand sides, so rows are exchanged over their full width (LAPACK
+// order): P A = L' U', solved as y = L'^{-1} P r, d = U'^{-1} y.
+//
+// One CTA per system from a largest-first queue, as in the FP64 variant.
+// Systems whose FP32 matrix fits shared memory are factored and solved
+// there; larger ones are factored blocked in their FP32 slot of the work
+// arena (panel of pw columns in shared memory) and solved from it.
+#include <climits>
+
+#include "lu2gpu_internal.cuh"
+
+namespace lu2gpu {
+
+__device__ __forceinline__ void ir_block_argmax(double &v, int &i, double *s_v, int *s_i)
+{
+    warp_argmax(v, i);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    if (lane == 0) {
+        s_v[warp] = v;
+        s_i[warp] = i;
+    }
+    __syncthreads();
+    v = lane < nw ? s_v[lane] : -1.0;
+    i = lane < nw ? s_i[lane] : INT_MAX;
+    warp_argmax(v, i);
+    __syncthreads();
+}
+
+// FP32 factorization of F (n x n, stride n) held in shared memory
+__device__ void ir_factor_smem(float *F, int n, int *piv, int *first_zero, double *s_v, int *s_i)
+{
+    const int T = blockDim.x, tid = threadIdx.x;
+    for (int k = 0; k < n; k++) {
+        double v = -1.0;
+        int p = INT_MAX;
+        for (int r = k + tid; r < n; r += T) {
+            const double a = fabsf(F[r * n + k]);
+            if (a > v) {
+                v = a;
+                p = r;
+            }
+        }
+        ir_block_argmax(v, p, s_v, s_i);
+        if (p == INT_MAX) p = k;
+        if (tid == 0) piv[k] = p;
+        if (p != k)
+            for (int c = tid; c < n; c += T) {
+                const float t = F[k * n + c];
+                F[k * n + c] = F[p * n + c];
+                F[p * n + c] = t;
+            }
+        __syncthreads();
+        const float d = F[k * n + k];
+        if (d == 0.f) {
+            if (!*first_zero && tid == 0) *first_zero = k + 1;
+            __syncthreads();
+            continue;
+        }
+        const float inv = 1.f / d;
+        for (int c = k + 1 + tid; c < n; c += T) F[k * n + c] *= inv;
+        __syncthreads();
+        const int w = n - k - 1;
+        for (int idx = tid; idx < w * w; idx += T) {
+            const int r = k + 1 + idx / w, c = k + 1 + idx % w;
+            F[r * n + c] -= F[r * n + k] * F[k * n + c];
+        }
+        __syncthreads();
+    }
+}
+
+// FP32 factorization of F (n x n, stride n) in global memory, panel of pw
+// columns staged in shared memory (P: rows x pw, U: pw x 64)
+__device__ void ir_factor_blocked(float *F, int n, int pw, float *P, float *U, int *piv, float *dinv,
+                                  int *first_zero, double *s_v, int *s_i)
+{
+    const int T = blockDim.x, tid = threadIdx.x;
+    for (int k0 = 0; k0 < n; k0 += pw) {
+        const int w = min(pw, n - k0), rows = n - k0;
+        for (int idx = tid; idx < rows * w; idx += T) {
+            const int r = idx / w, c = idx - r * w;
+            P[r * pw + c] = F[(size_t)(k0 + r) * n + k0 + c];
+        }
+        __syncthreads();
+        for (int c = 0; c < w; c++) {
+            double v = -1.0;
+            int p = INT_MAX;
+            for (int r = c + tid; r < rows; r += T) {
+                const double a = fabsf(P[r * pw + c]);
+                if (a > v) {
+                    v = a;
+                    p = r;
+                }
+            }
+            ir_block_argmax(v, p, s_v, s_i);
+            if (p == INT_MAX) p = c;
+            if (tid == 0) piv[k0 + c] = k0 + p;
+            if (p != c)
+                for (int j = tid; j < w; j += T) {
+                    const float t = P[c * pw + j];
+                    P[c * pw + j] = P[p * pw + j];
+                    P[p * pw + j] = t;
+                }
+            __syncthreads();
+            const float d = P[c * pw + c];
+            const bool zero = (d == 0.f);
+            if (zero && !*first_zero && tid == 0) *first_zero = k0 + c + 1;
+            const float inv = zero ? 1.f : 1.f / d;
+            if (tid == 0) dinv[c] = inv;
+            if (!zero)
+                for (int j = c + 1 + tid; j < w; j += T) P[c * pw + j] *= inv;
+            __syncthreads();
+            if (!zero) {
+                const int wj = w - c - 1, hr = rows - c - 1;
+                for (int idx = tid; idx < hr * wj; idx += T) {
+                    const int r = c + 1 + idx / wj, j = c + 1 + idx % wj;
+                    P[r * pw + j] -= P[r * pw + c] * P[c * pw + j];
+                }
+            }
+            __syncthreads();
+        }
+        for (int idx = tid; idx < rows * w; idx += T) {
+            const int r = idx / w, c = idx - r * w;
+            F[(size_t)(k0 + r) * n + k0 + c] = P[r * pw + c];
+        }
+        // exchanges of the earlier panels' columns (full-width rows), one thread per column
+        for (int j = tid; j < k0; j += T)
+            for (int c = 0; c < w; c++) {
+                const int p = piv[k0 + c];
+                if (p != k0 + c) {
+                    float *a = F + (size_t)(k0 + c) * n + j, *b = F + (size_t)p * n + j;
+                    const float t = *a;
+                    *a = *b;
+                    *b = t;
+                }
+            }
+        __syncthreads();
+        // right part: exchanges, then U' rows of the block (one thread per column)
+        const int cs = k0 + w;
+        for (int j = cs + tid; j < n; j += T) {
+            float x[64];
+            for (int c = 0; c < w; c++) {
+                const int p = piv[k0 + c];
+                float *rc = F + (size_t)(k0 + c) * n + j;
+                float vc = *rc;
+                if (p != k0 + c) {
+                    float *rp = F + (size_t)p * n + j;
+                    const float vp = *rp;
+                    *rp = vc;
+                    vc = vp;
+                }
+                x[c] = vc;
+            }
+            for (int r = 0; r < w; r++) {
+                float s = x[r];
+                for (int l = 0; l < r; l++) s -= P[r * pw + l] * x[l];
+                x[r] = s * dinv[r];
+            }
+            for (int c = 0; c < w; c++) F[(size_t)(k0 + c) * n + j] = x[c];
+        }
+        __syncthreads();
+        // trailing update F[cs.., cs..] -= L21 U12 in 64-column chunks
+        const int h = n - cs;
+        for (int c0 = cs; c0 < n && h > 0; c0 += 64) {
+            const int cw = min(64, n - c0);
+            for (int idx = tid; idx < w * 64; idx += T) {
+                const int l = idx >> 6, c = idx & 63;
+                U[l * 64 + c] = (c < cw) ? F[(size_t)(k0 + l) * n + c0 + c] : 0.f;
+            }
+            __syncthreads();
+            const int tx = tid & 15, ty = tid >> 4, tys = T >> 4;
+            for (int rb = ty * 4; rb < h; rb += tys * 4) {
+                float acc[4][4] = {};
+                for (int l = 0; l < w; l++) {
+                    float av[4], bv[4];
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        av[i] = (rb + i < h) ? P[(w + rb + i) * pw + l] : 0.f;
+                        bv[i] = U[l * 64 + tx * 4 + i];
+                    }
+#pragma unroll
+                    for (int i = 0; i < 4; i++)
+#pragma unroll
+                        for (int q = 0; q < 4; q++) acc[i][q] = fmaf(av[i], bv[q], acc[i][q]);
+                }
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    if (rb + i >= h) break;
+                    float *row = F + (size_t)(cs + rb + i) * n + c0;
+#pragma unroll
+                    for (int q = 0; q < 4; q++)
+                        if (tx * 4 + q < cw) row[tx * 4 + q] -= acc[i][q];
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// V (n x r, row-major, shared memory) = U'^{-1} L'^{-1} P V with the FP32 factors F
+// (stride n, shared or global memory); blocks of 32 rows: one warp solves the
+// diagonal block, every thread updates the rows beyond it
+__device__ void ir_solve(const float *F, int n, const int *piv, float *V, int r)
+{
+    const int T = blockDim.x, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    for (int q = tid; q < r; q += T)
+        for (int k = 0; k < n; k++) {
+            const int p = piv[k];
+            if (p != k) {
+                const float t = V[k * r + q];
+                V[k * r + q] = V[p * r + q];
+                V[p * r + q] = t;
+            }
+        }
+    __syncthreads();
+    // forward: y_k = (v_k - sum_{j<k} L'_kj y_j) / L'_kk
+    for (int b0 = 0; b0 < n; b0 += 32) {
+        const int bw = min(32, n - b0);
+        if (warp == 0)
+            for (int q = 0; q < r; q++) {
+                float v = lane < bw ? V[(b0 + lane) * r + q] : 0.f;
+                for (int k = 0; k < bw; k++) {
+                    float yk = __shfl_sync(0xffffffffu, v, k);
+                    yk /= F[(size_t)(b0 + k) * n + b0 + k];
+                    if (lane == k) v = yk;
+                    if (lane > k && lane < bw) v -= F[(size_t)(b0 + lane) * n + b0 + k] * yk;
+                }
+                if (lane < bw) V[(b0 + lane) * r + q] = v;
+            }
+        __syncthreads();
+        for (int idx = tid; idx < (n - b0 - bw) * r; idx += T) {
+            const int i = b0 + bw + idx / r, q = idx % r;
+            const float *row = F + (size_t)i * n + b0;
+            float s = 0.f;
+            for (int k = 0; k < bw; k++) s = fmaf(row[k], V[(b0 + k) * r + q], s);
+            V[i * r + q] -= s;
+        }
+        __syncthreads();
+    }
+    // backward: x_k = y_k - sum_{j>k} U'_kj x_j
+    for (int be = n; be > 0; be -= 32) {
+        const int b0 = max(0, be - 32), bw = be - b0;
+        if (warp == 0)
+            for (int q = 0; q < r; q++) {
+                float v = lane < bw ? V[(b0 + lane) * r + q] : 0.f;
+                for (int k = bw - 1; k >= 0; k--) {
+                    const float xk = __shfl_sync(0xffffffffu, v, k);
+                    if (lane < k) v -= F[(size_t)(b0 + lane) * n + b0 + k] * xk;
+                }
+                if (lane < bw) V[(b0 + lane) * r + q] = v;
+            }
+        __syncthreads();
+        for (int idx = tid; idx < b0 * r; idx += T) {
+            const int i = idx / r, q = idx % r;
+            const float *row = F + (size_t)i * n + b0;
+            float s = 0.f;
+            for (int k = 0; k < bw; k++) s = fmaf(row[k], V[(b0 + k) * r + q], s);
+            V[i * r + q] -= s;
+        }
+        __syncthreads();
+    }
+}
+
+// R = B - A X (FP64, warp per row) and the HPL norms: per right-hand side
+// max|r|, max|x|; with `first`, also max|b| and ||A||_inf
+__device__ void ir_residual(const double *A, long ld, int n, int r, const double *X, double *R, bool first,
+                            double *s_red, double *rmax, double *xmax, double *bmax, double *anorm)
+{
+    const int T = blockDim.x, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = T >> 5;
+    double my_r[IR_MAX_RHS], my_b[IR_MAX_RHS], my_a = 0.0;
+    for (int q = 0; q < IR_MAX_RHS; q++) my_r[q] = my_b[q] = 0.0;
+    for (int i = warp; i < n; i += nw) {
+        const double *row = A + (size_t)i * ld;
+        double s[IR_MAX_RHS], sa = 0.0;
+        for (int q = 0; q < IR_MAX_RHS; q++) s[q] = 0.0;
+        for (int j = lane; j < n; j += 32) {
+            const double a = row[j];
+            sa += fabs(a);
+            for (int q = 0; q < r; q++) s[q] = fma(a, X[(size_t)j * r + q], s[q]);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            sa += __shfl_xor_sync(0xffffffffu, sa, o);
+            for (int q = 0; q < r; q++) s[q] += __shfl_xor_sync(0xffffffffu, s[q], o);
+        }
+        if (lane == 0) {
+            my_a = fmax(my_a, sa);
+            for (int q = 0; q < r; q++) {
+                const double b = row[n + q];
+                const double res = b - s[q];
+                R[(size_t)i * r + q] = res;
+                my_r[q] = fmax(my_r[q], fabs(res));
+                my_b[q] = fmax(my_b[q], fabs(b));
+            }
+        }
+    }
+    // block maxima (lane 0 of every warp holds partials); s_red: 32 x (2 r + 1)
+    const int stride = 2 * IR_MAX_RHS + 1;
+    if (lane == 0) {
+        for (int q = 0; q < r; q++) {
+            s_red[warp * stride + q] = my_r[q];
+            s_red[warp * stride + IR_MAX_RHS + q] = my_b[q];
+        }
+        s_red[warp * stride + 2 * IR_MAX_RHS] = my_a;
+    }
+    __syncthreads();
+    if (tid < r) {
+        double m1 = 0.0, m2 = 0.0, m3 = 0.0;
+        for (int w = 0; w < nw; w++) {
+            m1 = fmax(m1, s_red[w * stride + tid]);
+            m2 = fmax(m2, s_red[w * stride + IR_MAX_RHS + tid]);
+            m3 = fmax(m3, s_red[w * stride + 2 * IR_MAX_RHS]);
+        }
+        rmax[tid] = m1;
+        if (first) {
+            bmax[tid] = m2;
+            if (tid == 0) *anorm = m3;
+        }
+        double xm = 0.0;
+        for (int i = 0; i < n; i++) xm = fmax(xm, fabs(X[(size_t)i * r + tid]));
+        xmax[tid] = xm;
+    }
+    __syncthreads();
+}
+
+__global__ void batch_ir_kernel(double *data, const BatchSys *sys, const long long *woff, uint8_t *arena,
+                                const int *order, int count, int *counter, int *info, int *iters, int pw,
+                                long smem_floats, int max_iter)
+{
+    extern __shared__ float ism[];
+    __shared__ double s_v[32];
+    __shared__ int s_i[32];
+    __shared__ int s_next, s_zero, s_done;
+    __shared__ float s_dinv[64];
+    __shared__ double s_red[32 * (2 * IR_MAX_RHS + 1)];
+    __shared__ double s_rmax[IR_MAX_RHS], s_xmax[IR_MAX_RHS], s_bmax[IR_MAX_RHS], s_anorm;
+    const int T = blockDim.x, tid = threadIdx.x;
+    for (;;) {
+        if (tid == 0) s_next = atomicAdd(counter, 1);
+        __syncthreads();
+        const int qi = s_next;
+        __syncthreads();
+        if (qi >= count) break;
+        const int si = order[qi];
+        const BatchSys S = sys[si];
+        const int n = S.n, r = S.nrhs;
+        double *A = data + S.off;
+        uint8_t *w = arena + woff[si];
+        float *Fg = reinterpret_cast<float *>(w);
+        int *piv = reinterpret_cast<int *>(w + ir_align16((size_t)n * n * 4));
+        double *X = reinterpret_cast<double *>(w + ir_align16((size_t)n * n * 4) + ir_align16((size_t)n * 4));
+        double *R = X + (size_t)n * r;
+        const bool in_smem = (long)n * n + (long)n * r <= smem_floats;
+        float *F = in_smem ? ism : Fg;
+        float *V = in_smem ? ism + (size_t)n * n : ism + (size_t)n * pw + (size_t)pw * 64;
+        if (tid == 0) s_zero = 0;
+        for (int idx = tid; idx < n * n; idx += T) {
+            const int i = idx / n, j = idx - i * n;
+            F[idx] = (float)A[(size_t)i * S.ld + j];
+        }
+        __syncthreads();
+        if (in_smem)
+            ir_factor_smem(F, n, piv, &s_zero, s_v, s_i);
+        else
+            ir_factor_blocked(F, n, pw, ism, ism + (size_t)n * pw, piv, s_dinv, &s_zero, s_v, s_i);
+        __syncthreads();
+        int it = 0;
+        if (s_zero == 0) {
+            // x_0 = 0, r_0 = b
+            for (int idx = tid; idx < n * r; idx += T) {
+                const int i = idx / r, q = idx - i * r;
+                X[idx] = 0.0;
+                R[idx] = A[(size_t)i * S.ld + n + q];
+            }
+            __syncthreads();
+            ir_residual(A, S.ld, n, r, X, R, true, s_red, s_rmax, s_xmax, s_bmax, &s_anorm);
+            for (it = 1; it <= max_iter; it++) {
+                for (int idx = tid; idx < n * r; idx += T) V[idx] = (float)R[idx];
+                __syncthreads();
+                ir_solve(F, n, piv, V, r);
+                for (int idx = tid; idx < n * r; idx += T) X[idx] += (double)V[idx];
+                __syncthreads();
+                ir_residual(A, S.ld, n, r, X, R, false, s_red, s_rmax, s_xmax, s_bmax, &s_anorm);
+                if (tid == 0) {
+                    bool ok = true;
+                    for (int q = 0; q < r; q++) {
+                        const double h = s_rmax[q] / (1.1102230246251565e-16 * (s_anorm * s_xmax[q] + s_bmax[q]) * n);
+                        if (!(h < 16.0)) ok = false;
+                    }
+                    s_done = ok;
+                }
+                __syncthreads();
+                if (s_done) break;
+            }
+            if (it > max_iter) it = max_iter;
+            for (int idx = tid; idx < n * r; idx += T) {
+                const int i = idx / r, q = idx - i * r;
+                A[(size_t)i * S.ld + n + q] = X[idx];
+            }
+        }
+        if (tid == 0) {
+            info[si] = s_zero;
+            iters[si] = it;
+        }
+        __syncthreads();
+    }
+}
+
+long batch_ir_smem_floats(const BatchSys *sys, int count, int pw, long floor_floats)
+{
+    long need = floor_floats;
+    for (int i = 0; i < count; i++) {
+        const long b = (long)sys[i].n * pw + (long)pw * 64 + (long)sys[i].n * sys[i].nrhs;
+        if (b > need) need = b;
+    }
+    return need;
+}
+
+cudaError_t batch_ir_grid(int threads, long smem_floats, int ctas_per_sm, int count, int *grid)
+{
+    if (threads < 64 || threads > 1024 || (threads & 31)) return cudaErrorInvalidValue;
+    const size_t smem = (size_t)smem_floats * sizeof(float);
+    if (smem > BATCH_SMEM_MAX) return cudaErrorInvalidValue;
+    cudaError_t e = cudaFuncSetAttribute(batch_ir_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, BATCH_SMEM_MAX);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 148;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    int occ = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_ir_kernel, threads, smem)) != cudaSuccess)
+        return e;
+    if (occ < 1) return cudaErrorInvalidConfiguration;
+    if (ctas_per_sm > occ || ctas_per_sm < 1) ctas_per_sm = occ;
+    const int g = sms * ctas_per_sm;
+    *grid = g > count ? count : g;
+    return cudaSuccess;
+}
+
+cudaError_t launch_batch_ir(double *data, const BatchSys *sys, const long long *woff, uint8_t *arena,
+                            const int *order, int count, int *counter, int *info, int *iters, long smem_floats, int pw,
+                            int threads, int grid, int max_iter, cudaStream_t st)
+{
+    if (count <= 0) return cudaSuccess;
+    if (pw < 16 || pw > 64 || threads < 64 || threads > 1024 || (threads & 31) || grid < 1 || max_iter < 1 ||
+        (size_t)smem_floats * sizeof(float) > BATCH_SMEM_MAX)
+        return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), st);
+    if (e != cudaSuccess) return e;
+    count_launch();
+    batch_ir_kernel<<<grid, threads, (size_t)smem_floats * sizeof(float), st>>>(
+        data, sys, woff, arena, order, count, counter, info, iters, pw, smem_floats, max_iter);
+    return cudaGetLastError();
+}
+
+}  // namespace lu2gpu

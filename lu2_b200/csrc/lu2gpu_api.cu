@@ -1532,6 +1532,12 @@ struct lu2gpu_batch {
     int threads = 256, pw = 32, ctas_per_sm = 1;
     long smem_doubles = 0;
     int grid = 0;
+    // FP32-LU + FP64 refinement variant
+    int mode = LU2GPU_BATCH_FP64, max_iter = 10;
+    long long *d_woff = nullptr;
+    uint8_t *d_arena = nullptr;
+    int *d_iters = nullptr;
+    long smem_floats = 0;
     cudaStream_t capture = nullptr;  // private stream the graph is captured on
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -1548,6 +1554,31 @@ static void batch_drop_graph(lu2gpu_batch *b)
 // adopt a launch shape if every system of the batch fits it; 0 or an error status
 static int batch_configure(lu2gpu_batch *b, int threads, int pw, int ctas_per_sm)
 {
+    if (b->mode == LU2GPU_BATCH_FP32_IR) {
+        // the FP32 variant keeps as many systems as fit entirely in shared memory
+        const long floor_floats = (long)(BATCH_SMEM_MAX / sizeof(float)) / (ctas_per_sm > 1 ? 2 : 1);
+        const long sf = batch_ir_smem_floats(b->sys.data(), b->count, pw, floor_floats);
+        if ((size_t)sf * sizeof(float) > BATCH_SMEM_MAX) {
+            set_error("batch: panel width %d needs %ld bytes of shared memory for n=%d (limit %zu)", pw,
+                      sf * (long)sizeof(float), b->max_n, BATCH_SMEM_MAX);
+            return LU2GPU_ERR_ARG;
+        }
+        int grid = 0;
+        cudaError_t e = batch_ir_grid(threads, sf, ctas_per_sm, b->count, &grid);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            set_error("batch: launch shape threads=%d pw=%d ctas=%d not launchable: %s", threads, pw, ctas_per_sm,
+                      cudaGetErrorString(e));
+            return LU2GPU_ERR_ARG;
+        }
+        b->threads = threads;
+        b->pw = pw;
+        b->ctas_per_sm = ctas_per_sm;
+        b->smem_floats = sf;
+        b->grid = grid;
+        batch_drop_graph(b);
+        return 0;
+    }
     const long sd = batch_smem_doubles(b->sys.data(), b->count, pw);
     if ((size_t)sd * sizeof(double) > BATCH_SMEM_MAX) {
         set_error("batch: panel width %d needs %ld bytes of shared memory for n=%d (limit %zu)", pw,
@@ -1584,6 +1615,9 @@ extern "C" int lu2gpu_batch_destroy(lu2gpu_batch *b)
     cudaFree(b->d_data);
     cudaFree(b->d_orig);
     cudaFree(b->d_resid);
+    cudaFree(b->d_woff);
+    cudaFree(b->d_arena);
+    cudaFree(b->d_iters);
     if (b->capture) cudaStreamDestroy(b->capture);
     delete b;
     return 0;
@@ -1697,8 +1731,71 @@ extern "C" int lu2gpu_batch_restore(lu2gpu_batch *b)
 
 static int batch_enqueue(lu2gpu_batch *b, cudaStream_t st)
 {
+    if (b->mode == LU2GPU_BATCH_FP32_IR) {
+        K_TRY(launch_batch_ir(b->d_data, b->d_sys, b->d_woff, b->d_arena, b->d_order, b->count, b->d_counter,
+                              b->d_info, b->d_iters, b->smem_floats, b->pw, b->threads, b->grid, b->max_iter, st));
+        return 0;
+    }
     K_TRY(launch_batch_lu(b->d_data, b->d_sys, b->d_order, b->count, b->d_counter, b->d_info, b->smem_doubles, b->pw,
                           b->threads, b->grid, st));
+    return 0;
+}
+
+// Select the arithmetic of lu2gpu_batch_solve: plain FP64, or FP32 factors
+// with FP64 refinement (nrhs <= 8 per system) of at most max_iter corrections.
+extern "C" int lu2gpu_batch_set_mode(lu2gpu_batch *b, int mode, int max_iter)
+{
+    if (!b || (mode != LU2GPU_BATCH_FP64 && mode != LU2GPU_BATCH_FP32_IR) || max_iter < 1) {
+        set_error("lu2gpu_batch_set_mode: bad arguments");
+        return LU2GPU_ERR_ARG;
+    }
+    DeviceGuard g(b->ctx->device);
+    if (mode == LU2GPU_BATCH_FP32_IR && !b->d_arena) {
+        std::vector<long long> woff(b->count);
+        size_t off = 0;
+        for (int i = 0; i < b->count; i++) {
+            if (b->sys[i].nrhs > IR_MAX_RHS) {
+                set_error("lu2gpu_batch_set_mode: system %d has %d right-hand sides (at most %d with refinement)", i,
+                          b->sys[i].nrhs, IR_MAX_RHS);
+                return LU2GPU_ERR_ARG;
+            }
+            woff[i] = (long long)off;
+            off += ir_slot_bytes(b->sys[i].n, b->sys[i].nrhs);
+        }
+        if (cudaMalloc(&b->d_woff, sizeof(long long) * b->count) != cudaSuccess ||
+            cudaMalloc(&b->d_arena, off + 256) != cudaSuccess ||
+            cudaMalloc(&b->d_iters, sizeof(int) * b->count) != cudaSuccess) {
+            cudaGetLastError();
+            cudaFree(b->d_woff);
+            cudaFree(b->d_arena);
+            cudaFree(b->d_iters);
+            b->d_woff = nullptr;
+            b->d_arena = nullptr;
+            b->d_iters = nullptr;
+            set_error("lu2gpu_batch_set_mode: device allocation of %zu bytes failed", off);
+            return LU2GPU_ERR_NOMEM;
+        }
+        CU_TRY(cudaMemcpy(b->d_woff, woff.data(), sizeof(long long) * b->count, cudaMemcpyHostToDevice));
+        CU_TRY(cudaMemset(b->d_iters, 0, sizeof(int) * b->count));
+    }
+    const int old = b->mode;
+    b->mode = mode;
+    b->max_iter = max_iter;
+    int rc = batch_configure(b, 256, 32, 1);
+    if (rc) rc = batch_configure(b, 256, 16, 1);
+    if (rc) b->mode = old;
+    return rc;
+}
+
+// Refinement corrections each system took in the last FP32-IR solve.
+extern "C" int lu2gpu_batch_iterations(lu2gpu_batch *b, int *iters_host)
+{
+    if (!b || !iters_host || !b->d_iters) {
+        set_error("lu2gpu_batch_iterations: no FP32-IR solve on this batch");
+        return LU2GPU_ERR_ARG;
+    }
+    DeviceGuard g(b->ctx->device);
+    CU_TRY(cudaMemcpy(iters_host, b->d_iters, sizeof(int) * b->count, cudaMemcpyDeviceToHost));
     return 0;
 }
 

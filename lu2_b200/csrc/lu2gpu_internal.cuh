@@ -196,6 +196,21 @@ cudaError_t launch_batch_lu(double *data, const BatchSys *sys, const int *order,
                             long smem_doubles, int pw, int threads, int grid, cudaStream_t st);
 cudaError_t launch_batch_residual(const double *orig, const double *solved, const BatchSys *sys, int count,
                                   double *out, cudaStream_t st);
+
+// FP32-LU + FP64 refinement variant (kernels_batch_ir.cu).  Work arena slot
+// of a system: FP32 factors (n x n), pivots (n), x and r (n x nrhs doubles).
+constexpr int IR_MAX_RHS = 8;
+__host__ __device__ inline size_t ir_align16(size_t b) { return (b + 15) & ~(size_t)15; }
+__host__ __device__ inline size_t ir_slot_bytes(int n, int nrhs)
+{
+    return ir_align16((size_t)n * n * 4) + ir_align16((size_t)n * 4) + (size_t)16 * n * nrhs;
+}
+// shared-memory floats a CTA needs: the blocked path of every system, at least floor_floats
+long batch_ir_smem_floats(const BatchSys *sys, int count, int pw, long floor_floats);
+cudaError_t batch_ir_grid(int threads, long smem_floats, int ctas_per_sm, int count, int *grid);
+cudaError_t launch_batch_ir(double *data, const BatchSys *sys, const long long *woff, uint8_t *arena,
+                            const int *order, int count, int *counter, int *info, int *iters, long smem_floats, int pw,
+                            int threads, int grid, int max_iter, cudaStream_t st);
 cudaError_t launch_batch_generate(double *data, const BatchSys *sys, int count, unsigned long long seed_base,
                                   cudaStream_t st);
 // *out = max(*out, max |v|) as double bits

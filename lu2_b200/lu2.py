@@ -21,6 +21,8 @@ PIVOT_REF = 0
 PIVOT_PARTIAL = 1
 UPDATE_BF16 = 0
 UPDATE_FP8 = 1
+BATCH_FP64 = 0
+BATCH_FP32_IR = 1
 CBLAS_ROWMAJOR, CBLAS_COLMAJOR, CBLAS_NOTRANS, CBLAS_TRANS = 101, 102, 111, 112
 TIMER_NAMES = ["col dec t", "swaprows", "solve tri", "DGEMMrest", "backward_sub", "panel update"]
 
@@ -268,6 +270,15 @@ class Batch:
 
     def set_config(self, threads: int, pw: int, ctas_per_sm: int) -> None:
         _check("lu2gpu_batch_set_config", lib().lu2gpu_batch_set_config(self._h, threads, pw, ctas_per_sm))
+
+    def set_mode(self, mode: int, max_iter: int = 10) -> None:
+        """BATCH_FP64 or BATCH_FP32_IR (FP32 factors, FP64 refinement to HPL < 16)."""
+        _check("lu2gpu_batch_set_mode", lib().lu2gpu_batch_set_mode(self._h, mode, max_iter))
+
+    def iterations(self) -> np.ndarray:
+        out = np.zeros(self.count, dtype=np.int32)
+        _check("lu2gpu_batch_iterations", lib().lu2gpu_batch_iterations(self._h, _ptr(out)))
+        return out
 
     def autotune(self) -> dict:
         out = np.zeros(4, dtype=np.int32)

@@ -150,3 +150,61 @@ def test_batch_on_legacy_default_stream():
         assert (b.residuals() < 16).all()
     b.close()
     c.close()
+
+
+@pytest.fixture(scope="module")
+def ir_batch(ctx):
+    n, r = L.batch_sizes(300, 11, 16, 512, 0.1, 8)
+    b = L.Batch(ctx, n, r)
+    b.generate(2000)
+    b.snapshot()
+    b.set_mode(L.BATCH_FP32_IR, 10)
+    yield b
+    b.close()
+
+
+def test_batch_fp32_ir_reaches_fp64_residual(ctx, ir_batch):
+    """FP32 factors + FP64 refinement: every system (blocked and in-shared-
+    memory paths, 1 and 8 right-hand sides) reaches HPL < 16 and matches an
+    FP64 LAPACK solve."""
+    import scipy.linalg as sl
+
+    ir_batch.restore()
+    info = ir_batch.solve()
+    assert (info == 0).all()
+    res = ir_batch.residuals()
+    assert (res < 16).all(), res.max()
+    its = ir_batch.iterations()
+    assert its.min() >= 1 and its.max() <= 6, (its.min(), its.max())
+    for i in (0, 3, 150, 299):
+        n, r = int(ir_batch.n[i]), int(ir_batch.nrhs[i])
+        x = fetch(ir_batch, i)[:, n:n + r]
+        ir_batch.restore()
+        a0 = fetch(ir_batch, i)
+        xs = sl.solve(a0[:, :n], a0[:, n:n + r])
+        assert np.abs(x - xs).max() / np.abs(xs).max() < 1e-9
+        ir_batch.solve()
+
+
+@pytest.mark.parametrize("threads,pw,ctas", [(128, 16, 1), (512, 32, 1), (256, 16, 2)])
+def test_batch_fp32_ir_launch_shapes(ctx, ir_batch, threads, pw, ctas):
+    ir_batch.set_config(threads, pw, ctas)
+    ir_batch.restore()
+    assert (ir_batch.solve() == 0).all()
+    assert (ir_batch.residuals() < 16).all()
+
+
+def test_batch_fp32_ir_autotune_and_replay(ctx, ir_batch):
+    cfg = ir_batch.autotune()
+    assert cfg["threads"] in (128, 256, 512)
+    for _ in range(2):
+        ir_batch.restore()
+        assert (ir_batch.solve() == 0).all()
+        assert (ir_batch.residuals() < 16).all()
+
+
+def test_batch_fp32_ir_rejects_many_rhs(ctx):
+    b = L.Batch(ctx, np.array([32, 40], dtype=np.int32), np.array([1, 9], dtype=np.int32))
+    with pytest.raises(L.Lu2GpuError):
+        b.set_mode(L.BATCH_FP32_IR, 10)
+    b.close()
