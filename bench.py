@@ -22,8 +22,10 @@ cpu_baseline: the reference compiled from its own sources (oracle/_ref:
 
 --impl reference times that same reference CPU build on a bounded sample
 (N = 8192) of the workload, on rank 0 only.
-Multi-GPU (--gpus N under torchrun): independent replicas, one system per GPU
-(LU has no natural sharding at this scope), weak scaling.
+Multi-GPU (--gpus N under torchrun): the plain, BF16 and FP8 forms run as
+independent replicas, one system per GPU (LU has no natural sharding at this
+scope), weak scaling; the batched form splits its 20,000 systems over the GPUs
+by cost (strong scaling), with no data exchange.
 """
 from __future__ import annotations
 
@@ -245,7 +247,7 @@ def run_mixed(ctx, n, nb_fp64, ld, buf, dev, stream, args, barrier, max_over_ran
             "phases_ms": {k: {"ms": v[0], "launches": v[1]} for k, v in timers.items()}}
 
 
-def run_batched(ctx, dev, stream, args, max_over_ranks, world) -> dict:
+def run_batched(ctx, dev, stream, args, max_over_ranks, world, rank=0) -> dict:
     """Batching form: 20,000 systems, N log-uniform in [16, 512]
     (seed 1), 10% with 8 right-hand sides, each lu2's stream with seed 1+i; FP64,
     one persistent launch replayed from a CUDA graph, launch shape autotuned.
@@ -257,11 +259,14 @@ def run_batched(ctx, dev, stream, args, max_over_ranks, world) -> dict:
     import lu2_b200 as L
 
     count = args.batch_count
-    n, r = L.batch_sizes(count, 1, 16, 512, 0.1, 8)
+    n_all, r_all = L.batch_sizes(count, 1, 16, 512, 0.1, 8)
+    # on N GPUs every rank solves its cost-balanced share of the same systems
+    idx = L.batch_shard(n_all, r_all, world, rank) if world > 1 else np.arange(count)
+    n, r = n_all[idx], r_all[idx]
     b = L.Batch(ctx, n, r)
-    b.generate(1)
+    b.generate_seeds(1 + idx)
     b.snapshot()
-    flops = float(np.sum(2.0 / 3.0 * n.astype(np.float64) ** 3 + 2.0 * n.astype(np.float64) ** 2 * r))
+    flops = float(np.sum(2.0 / 3.0 * n_all.astype(np.float64) ** 3 + 2.0 * n_all.astype(np.float64) ** 2 * r_all))
 
     def timed():
         """autotune, warm up, time args.steps solves (inputs restored untimed)"""
@@ -286,15 +291,18 @@ def run_batched(ctx, dev, stream, args, max_over_ranks, world) -> dict:
     b.set_mode(L.BATCH_FP32_IR, 10)
     cfg_ir, t_ir, info_ir, res_ir, _ = timed()
     its = b.iterations()
-    fp32_ir = {"value": world * count / t_ir, "unit": "systems/s", "seconds": t_ir,
-               "fp64_equivalent_gflops": world * flops / t_ir / 1e9, "max_hpl_residual": float(res_ir.max()),
-               "all_below_16": bool((res_ir < 16).all()), "zero_pivots": int((info_ir != 0).sum()),
-               "refinement_iterations": {"mean": float(its.mean()), "max": int(its.max())}, "autotuned": cfg_ir}
+    hmax_ir = max_over_ranks(float(res_ir.max()))
+    fp32_ir = {"value": count / t_ir, "unit": "systems/s", "seconds": t_ir,
+               "fp64_equivalent_gflops": flops / t_ir / 1e9, "max_hpl_residual": hmax_ir,
+               "all_below_16": hmax_ir < 16, "zero_pivots_max_per_rank": max_over_ranks(float((info_ir != 0).sum())),
+               "refinement_iterations": {"mean": float(its.mean()), "max": int(max_over_ranks(float(its.max())))},
+               "autotuned": cfg_ir}
     b.set_mode(L.BATCH_FP64)
     cfg, t, info, res, nsteps = timed()
-    # the loop of single plain-method launches, on a sample of systems
+    hmax = max_over_ranks(float(res.max()))
+    # the loop of single plain-method launches, on a sample of this rank's systems
     rng = np.random.default_rng(0)
-    sample = rng.choice(count, size=min(args.batch_loop_sample, count), replace=False)
+    sample = rng.choice(len(idx), size=min(args.batch_loop_sample, len(idx)), replace=False)
     b.restore()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -302,16 +310,19 @@ def run_batched(ctx, dev, stream, args, max_over_ranks, world) -> dict:
         ptr, ld = b.system(int(i))
         ctx.lusolve(ptr, int(n[i]), ld, 64, int(r[i]), L.PIVOT_PARTIAL)
     torch.cuda.synchronize()
-    t_loop = (time.perf_counter() - t0) / len(sample)
+    t_loop = max_over_ranks((time.perf_counter() - t0) / len(sample))
     b.close()
-    sps = world * count / t
+    sps = count / t
     return {"metric": "batched solves/s", "value": sps, "unit": "systems/s", "seconds": t, "systems": count,
-            "gflops": world * flops / t / 1e9, "flops": flops,
+            "gflops": flops / t / 1e9, "flops": flops,
+            "scaling": "strong" if world > 1 else None,
+            "sharding": "cost-balanced split of the same %d systems over %d GPUs, no data exchange" % (count, world),
             "sizes": "N log-uniform in [16, 512] (seed 1), 10% with 8 right-hand sides, entries lu2 stream seed 1+i",
-            "max_hpl_residual": float(res.max()), "all_below_16": bool((res < 16).all()),
-            "zero_pivots": int((info != 0).sum()), "autotuned": cfg, "steps": nsteps, "warmup": args.warmup,
-            "loop_baseline": {"solves_per_s": 1.0 / t_loop, "sample_systems": int(len(sample)),
-                              "api": "lu2gpu_lusolve per system (nb=64), host-timed loop"},
+            "max_hpl_residual": hmax, "all_below_16": hmax < 16,
+            "zero_pivots_max_per_rank": max_over_ranks(float((info != 0).sum())), "autotuned": cfg, "steps": nsteps,
+            "warmup": args.warmup,
+            "loop_baseline": {"solves_per_s": world / t_loop, "sample_systems_per_rank": int(len(sample)),
+                              "api": "lu2gpu_lusolve per system (nb=64), host-timed loop on every GPU"},
             "speedup_vs_loop": sps / (world / t_loop), "fp32_lu_fp64_ir": fp32_ir}
 
 
@@ -648,7 +659,7 @@ def main() -> int:
         del pristine
     torch.cuda.empty_cache()
     if not args.no_batched:
-        forms["batched_fp64"] = run_batched(ctx, dev, stream, args, max_over_ranks, world)
+        forms["batched_fp64"] = run_batched(ctx, dev, stream, args, max_over_ranks, world, rank)
     if not args.no_fp8:
         forms["fp8_gmres_ir"] = run_fp8(ctx, dev, stream, args, max_over_ranks, world)
 

@@ -247,6 +247,9 @@ int lu2gpu_batch_destroy(lu2gpu_batch *b);
 int lu2gpu_batch_system(lu2gpu_batch *b, int i, double **a, long *ld);
 /* System i := lu2's randomsetmat stream with seed (seed + i). */
 int lu2gpu_batch_generate(lu2gpu_batch *b, long seed);
+/* System i := lu2's randomsetmat stream with seed seeds[i] (host, count
+ * seeds), so that a shard of a batch holds the same systems as the whole. */
+int lu2gpu_batch_generate_seeds(lu2gpu_batch *b, const long long *seeds);
 /* Keep a copy of the current systems (for residuals and for re-running). */
 int lu2gpu_batch_snapshot(lu2gpu_batch *b);
 int lu2gpu_batch_restore(lu2gpu_batch *b);

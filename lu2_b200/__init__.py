@@ -15,6 +15,7 @@ from .lu2 import (  # noqa: F401
     Batch,
     Context,
     Lu2GpuError,
+    batch_shard,
     batch_sizes,
     device_ld,
     gdr_dgemm_,

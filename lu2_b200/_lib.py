@@ -64,6 +64,7 @@ SIGNATURES = {
     "lu2gpu_batch_destroy": (C.c_int, [vp]),
     "lu2gpu_batch_system": (C.c_int, [vp, C.c_int, C.POINTER(vp), C.POINTER(C.c_long)]),
     "lu2gpu_batch_generate": (C.c_int, [vp, C.c_long]),
+    "lu2gpu_batch_generate_seeds": (C.c_int, [vp, vp]),
     "lu2gpu_batch_snapshot": (C.c_int, [vp]),
     "lu2gpu_batch_restore": (C.c_int, [vp]),
     "lu2gpu_batch_set_config": (C.c_int, [vp, C.c_int, C.c_int, C.c_int]),

@@ -400,13 +400,16 @@ cudaError_t launch_batch_residual(const double *orig, const double *solved, cons
     return cudaGetLastError();
 }
 
-// system i of a batch: lu2's stream (randomsetmat) with seed base + i
-__global__ void batch_generate_kernel(double *data, const BatchSys *sys, int count, unsigned long long seed_base)
+// system i of a batch: lu2's stream (randomsetmat) with seed seeds[i], or
+// seed_base + i without a seed list
+__global__ void batch_generate_kernel(double *data, const BatchSys *sys, int count, unsigned long long seed_base,
+                                      const long long *seeds)
 {
     for (int i = blockIdx.x; i < count; i += gridDim.x) {
         const BatchSys S = sys[i];
         double *A = data + S.off;
-        const unsigned long long xs = (((seed_base + i) & 0xffffffffull) << 16) | 0x330Eull;
+        const unsigned long long seed = seeds ? (unsigned long long)seeds[i] : seed_base + i;
+        const unsigned long long xs = ((seed & 0xffffffffull) << 16) | 0x330Eull;
         const long total = (long)S.n * (S.n + 1) + (long)S.n * (S.nrhs - 1);
         for (long q = threadIdx.x; q < total; q += blockDim.x) {
             unsigned long long k = q + 1, aa = 1, cc = 0, ba = 0x5DEECE66Dull, bc = 0xBull;
@@ -436,11 +439,11 @@ __global__ void batch_generate_kernel(double *data, const BatchSys *sys, int cou
 }
 
 cudaError_t launch_batch_generate(double *data, const BatchSys *sys, int count, unsigned long long seed_base,
-                                  cudaStream_t st)
+                                  const long long *seeds, cudaStream_t st)
 {
     if (count <= 0) return cudaSuccess;
     count_launch();
-    batch_generate_kernel<<<count < 148 * 16 ? count : 148 * 16, 256, 0, st>>>(data, sys, count, seed_base);
+    batch_generate_kernel<<<count < 148 * 16 ? count : 148 * 16, 256, 0, st>>>(data, sys, count, seed_base, seeds);
     return cudaGetLastError();
 }
 

@@ -1697,9 +1697,35 @@ extern "C" int lu2gpu_batch_generate(lu2gpu_batch *b, long seed)
 {
     if (!b) return LU2GPU_ERR_ARG;
     DeviceGuard g(b->ctx->device);
-    K_TRY(launch_batch_generate(b->d_data, b->d_sys, b->count, (unsigned long long)seed, b->ctx->stream));
+    K_TRY(launch_batch_generate(b->d_data, b->d_sys, b->count, (unsigned long long)seed, nullptr, b->ctx->stream));
     CU_TRY(cudaStreamSynchronize(b->ctx->stream));
     return 0;
+}
+
+// System i := lu2's stream with seed seeds[i] (host list of count seeds): a
+// shard of a larger batch generates the same systems as the whole batch would.
+extern "C" int lu2gpu_batch_generate_seeds(lu2gpu_batch *b, const long long *seeds)
+{
+    if (!b || !seeds) {
+        set_error("lu2gpu_batch_generate_seeds: bad arguments");
+        return LU2GPU_ERR_ARG;
+    }
+    DeviceGuard g(b->ctx->device);
+    long long *d = nullptr;
+    if (cudaMalloc(&d, sizeof(long long) * b->count) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("lu2gpu_batch_generate_seeds: allocation failed");
+        return LU2GPU_ERR_NOMEM;
+    }
+    int rc = 0;
+    if (cudaMemcpy(d, seeds, sizeof(long long) * b->count, cudaMemcpyHostToDevice) != cudaSuccess ||
+        launch_batch_generate(b->d_data, b->d_sys, b->count, 0, d, b->ctx->stream) != cudaSuccess ||
+        cudaStreamSynchronize(b->ctx->stream) != cudaSuccess) {
+        set_error("lu2gpu_batch_generate_seeds: %s", cudaGetErrorString(cudaGetLastError()));
+        rc = LU2GPU_ERR_CUDA;
+    }
+    cudaFree(d);
+    return rc;
 }
 
 extern "C" int lu2gpu_batch_snapshot(lu2gpu_batch *b)

@@ -211,8 +211,9 @@ cudaError_t batch_ir_grid(int threads, long smem_floats, int ctas_per_sm, int co
 cudaError_t launch_batch_ir(double *data, const BatchSys *sys, const long long *woff, uint8_t *arena,
                             const int *order, int count, int *counter, int *info, int *iters, long smem_floats, int pw,
                             int threads, int grid, int max_iter, cudaStream_t st);
+// system i := lu2's randomsetmat stream with seed seeds[i] (device list) or seed_base + i
 cudaError_t launch_batch_generate(double *data, const BatchSys *sys, int count, unsigned long long seed_base,
-                                  cudaStream_t st);
+                                  const long long *seeds, cudaStream_t st);
 // *out = max(*out, max |v|) as double bits
 cudaError_t launch_vec_absmax(const double *v, int n, unsigned long long *out, cudaStream_t st);
 

@@ -230,6 +230,29 @@ def batch_sizes(count: int, seed: int, nmin: int = 16, nmax: int = 512, frac_mul
     return n, r
 
 
+def batch_shard(n, nrhs, world: int, rank: int) -> np.ndarray:
+    """Indices of the systems that rank `rank` of `world` solves.
+
+    The batching form shards without any exchange: the systems are
+    independent, so each GPU takes a share balanced by cost (2/3 n^3 + 2 n^2
+    nrhs FLOPs), assigned largest first to the least-loaded rank (ties to the
+    lowest rank).  Every rank computes the same split from the same sizes."""
+    import heapq
+
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("bad world/rank")
+    nf = np.asarray(n, dtype=np.float64)
+    rf = np.asarray(nrhs, dtype=np.float64)
+    cost = 2.0 / 3.0 * nf**3 + 2.0 * nf**2 * rf
+    owner = np.empty(len(nf), dtype=np.int64)
+    heap = [(0.0, k) for k in range(world)]
+    for i in np.argsort(-cost, kind="stable"):
+        load, k = heapq.heappop(heap)
+        owner[i] = k
+        heapq.heappush(heap, (load + cost[i], k))
+    return np.nonzero(owner == rank)[0]
+
+
 class Batch:
     """A batch of independent systems solved by one persistent launch."""
 
@@ -261,6 +284,13 @@ class Batch:
 
     def generate(self, seed: int) -> None:
         _check("lu2gpu_batch_generate", lib().lu2gpu_batch_generate(self._h, seed))
+
+    def generate_seeds(self, seeds) -> None:
+        """System i := lu2's stream with seed seeds[i]."""
+        s = np.ascontiguousarray(seeds, dtype=np.int64)
+        if s.shape != (self.count,):
+            raise ValueError("need one seed per system")
+        _check("lu2gpu_batch_generate_seeds", lib().lu2gpu_batch_generate_seeds(self._h, _ptr(s)))
 
     def snapshot(self) -> None:
         _check("lu2gpu_batch_snapshot", lib().lu2gpu_batch_snapshot(self._h))
