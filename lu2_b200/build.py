@@ -15,7 +15,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "liblu2gpu.so")
 SOURCES = ["kernels_leaf.cu", "kernels_panel.cu", "kernels_dgemm.cu", "kernels_solve.cu", "kernels_bf16.cu", "kernels_mixed.cu",
-           "kernels_batch.cu", "kernels_batch_ir.cu", "kernels_fp8.cu", "kernels_gmres.cu", "lu2gpu_api.cu"]
+           "kernels_batch.cu", "kernels_batch_ir.cu", "kernels_fp8.cu", "kernels_lowp.cu", "kernels_gmres.cu",
+           "lu2gpu_api.cu"]
 HEADERS = ["lu2gpu_internal.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

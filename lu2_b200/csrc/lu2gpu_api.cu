@@ -1438,8 +1438,8 @@ static int right_part32(lu2gpu_ctx *c, const View32 &v, int k0, int k1, int cs, 
             float *dqa = m->dq, *dqb = m->dq + (((size_t)M + 127) / 128) * (K / 128);
             K_TRY(launch_quant_fp8_tiles(L, v.ld, M, K, m->l8, K, dqa, c->stream));
             K_TRY(launch_quant_fp8_tiles(m->bt32top, K, N, K, m->b8, K, dqb, c->stream));
-            K_TRY(launch_fp8_update(m->l8, K, dqa, m->b8, K, dqb, v.a + (size_t)k1 * v.ld + cs, v.ld, M, N, K,
-                                    c->d_status, c->stream));
+            K_TRY(launch_lowp_update_fp8(m->l8, K, dqa, m->b8, K, dqb, v.a + (size_t)k1 * v.ld + cs, v.ld, M, N, K,
+                                         c->d_status, c->stream));
         }
         return 0;
     }
@@ -1457,8 +1457,8 @@ static int right_part32(lu2gpu_ctx *c, const View32 &v, int k0, int k1, int cs, 
         K_TRY(launch_panel_scales(m->amax(), m->scales(), c->stream));
         K_TRY(launch_f32_to_bf16(L, v.ld, m->l16, K, M, K, m->scales(), c->stream));
         K_TRY(launch_f32_transpose_bf16(X, v.ld, K, N, m->u16, m->scales() + 1, c->stream));
-        K_TRY(launch_bf16_update(m->l16, K, m->u16, K, v.a + (size_t)k1 * v.ld + cs, v.ld, M, N, K, m->scales() + 2,
-                                 c->d_status, c->stream));
+        K_TRY(launch_lowp_update_bf16(m->l16, K, m->u16, K, v.a + (size_t)k1 * v.ld + cs, v.ld, M, N, K,
+                                      m->scales() + 2, c->d_status, c->stream));
     }
     return 0;
 }
@@ -1513,7 +1513,7 @@ extern "C" int lu2gpu_bf16_update_dev(lu2gpu_ctx *c, int M, int N, int K, const 
     // the scale travels as a device scalar (the factorization computes it on the device)
     float *dscale = reinterpret_cast<float *>(c->d_bt);
     CU_TRY(cudaMemcpyAsync(dscale, &scale, sizeof(float), cudaMemcpyHostToDevice, c->stream));
-    K_TRY(launch_bf16_update(a16, lda, bt16, ldb, c32, ldc, M, N, K, dscale, c->d_status, c->stream));
+    K_TRY(launch_lowp_update_bf16(a16, lda, bt16, ldb, c32, ldc, M, N, K, dscale, c->d_status, c->stream));
     return end_status(c, "lu2gpu_bf16_update_dev");
 }
 
@@ -2275,6 +2275,6 @@ extern "C" int lu2gpu_fp8_update_dev(lu2gpu_ctx *c, int M, int N, int K, const f
     K_TRY(launch_quant_fp8_tiles(bt, ldb, N, K, b8, K, dqb, c->stream));
     if (a_deq) K_TRY(launch_dequant_fp8_tiles(a8, K, dqa, M, K, a_deq, K, c->stream));
     if (bt_deq) K_TRY(launch_dequant_fp8_tiles(b8, K, dqb, N, K, bt_deq, K, c->stream));
-    K_TRY(launch_fp8_update(a8, K, dqa, b8, K, dqb, c32, ldc, M, N, K, c->d_status, c->stream));
+    K_TRY(launch_lowp_update_fp8(a8, K, dqa, b8, K, dqb, c32, ldc, M, N, K, c->d_status, c->stream));
     return end_status(c, "lu2gpu_fp8_update_dev");
 }

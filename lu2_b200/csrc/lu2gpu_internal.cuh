@@ -142,12 +142,8 @@ cudaError_t launch_diag_inv(const double *a, long ld, int n, double *out, cudaSt
 cudaError_t launch_diag_inv(const float *a, long ld, int n, float *out, cudaStream_t st);
 
 // ---------------------------------------------------------------------------
-// precision form (kernels_bf16.cu, kernels_mixed.cu)
+// precision form (kernels_bf16.cu, kernels_mixed.cu; the trailing update in kernels_lowp.cu)
 
-// C (FP32, M x N, row-major) -= *scale * A Bt^T with A (M x K) and Bt (N x K)
-// BF16, K-contiguous, K a multiple of 64 and <= 256; tcgen05 (kind::f16).
-cudaError_t launch_bf16_update(const void *a_bf16, long lda, const void *bt_bf16, long ldb, float *c, long ldc, int M,
-                               int N, int K, const float *scale, int *status, cudaStream_t st);
 // out = BF16(in * *scale) for a rows x cols FP32 block
 cudaError_t launch_f32_to_bf16(const float *in, long ldi, void *out, long ldo, int rows, int cols,
                                const float *scale, cudaStream_t st);
@@ -217,11 +213,17 @@ cudaError_t launch_batch_generate(double *data, const BatchSys *sys, int count, 
 // *out = max(*out, max |v|) as double bits
 cudaError_t launch_vec_absmax(const double *v, int n, unsigned long long *out, cudaStream_t st);
 
-// FP8 form (kernels_fp8.cu): C (FP32) -= sum_kb da(tile_m,kb) db(tile_n,kb) Aq_kb Bq_kb^T with
-// E4M3 operands a8 (M x K, row stride lda bytes) and bt8 (N x K), K = 128 or 256
-cudaError_t launch_fp8_update(const uint8_t *a8, long lda, const float *da, const uint8_t *bt8, long ldb,
-                              const float *db, float *c, long ldc, int M, int N, int K, int *status, cudaStream_t st);
-// per-128x128-tile E4M3 quantization with power-of-two scales; dq = [ceil(rows/128)][cols/128]
+// persistent warp-specialized trailing update of the precision forms
+// (kernels_lowp.cu): C (FP32, 16-byte aligned, ldc a multiple of 4) -=
+// *scale * A Bt^T with BF16 operands (K a multiple of 64, <= 256), or
+// -= sum_kb da db Aq_kb Bq_kb^T with E4M3 operands and per-tile scales (K = 128 or 256)
+cudaError_t launch_lowp_update_bf16(const void *a16, long lda, const void *bt16, long ldb, float *c, long ldc, int M,
+                                    int N, int K, const float *scale, int *status, cudaStream_t st);
+cudaError_t launch_lowp_update_fp8(const uint8_t *a8, long lda, const float *da, const uint8_t *bt8, long ldb,
+                                   const float *db, float *c, long ldc, int M, int N, int K, int *status,
+                                   cudaStream_t st);
+
+// FP8 form operands (kernels_fp8.cu): per-128x128-tile E4M3 quantization with power-of-two scales; dq = [ceil(rows/128)][cols/128]
 cudaError_t launch_quant_fp8_tiles(const float *x, long ldx, int rows, int cols, uint8_t *q, long ldq, float *dq,
                                    cudaStream_t st);
 cudaError_t launch_dequant_fp8_tiles(const uint8_t *q, long ldq, const float *dq, int rows, int cols, float *y,
