@@ -81,6 +81,9 @@ struct lu2gpu_ctx {
     // staging for the host-pointer entry points
     double *d_stage[4] = {nullptr, nullptr, nullptr, nullptr};
     size_t stage_cap[4] = {0, 0, 0, 0};
+    // copies of finished factor blocks to pinned host memory during the factorization
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t copy_ev = nullptr;
     // phase timers
     bool timing = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[PH_COUNT];
@@ -197,6 +200,11 @@ extern "C" int lu2gpu_destroy(lu2gpu_ctx *c)
     cudaFree(c->d_ipiv);
     cudaFree(c->d_dinv);
     for (int i = 0; i < 4; i++) cudaFree(c->d_stage[i]);
+    if (c->copy_stream) {
+        cudaStreamSynchronize(c->copy_stream);
+        cudaStreamDestroy(c->copy_stream);
+    }
+    if (c->copy_ev) cudaEventDestroy(c->copy_ev);
     free_mixed(c);
     for (int p = 0; p < PH_COUNT; p++)
         for (auto &e : c->ev[p]) {
@@ -448,7 +456,13 @@ static int gpu_panel_width(int m)
     return w;
 }
 
-static int factor_enqueue(lu2gpu_ctx *c, int n, int nrhs, double *a, long lda, int nb, int mode)
+// `after_step(i, w)`, if given, runs once the enqueue of panel step i..i+w-1
+// is complete (rows i..i+w-1 from column i, and columns i..i+w-1 below them,
+// hold their final values once that work has executed: later steps touch
+// neither, lu2.c:543-553)
+template <typename AfterStep>
+static int factor_enqueue_with(lu2gpu_ctx *c, int n, int nrhs, double *a, long lda, int nb, int mode,
+                               AfterStep after_step)
 {
     if (nb > NB_MAX) nb = NB_MAX;
     int rc = ensure_work(c, n, n + nrhs, nb);
@@ -460,8 +474,14 @@ static int factor_enqueue(lu2gpu_ctx *c, int n, int nrhs, double *a, long lda, i
         if (rc) return rc;
         rc = right_part(c, v, i, i + w, i + w, n + nrhs, true);
         if (rc) return rc;
+        if ((rc = after_step(i, w))) return rc;
     }
     return 0;
+}
+
+static int factor_enqueue(lu2gpu_ctx *c, int n, int nrhs, double *a, long lda, int nb, int mode)
+{
+    return factor_enqueue_with(c, n, nrhs, a, lda, nb, mode, [](int, int) { return 0; });
 }
 
 extern "C" int lu2gpu_factor(lu2gpu_ctx *c, int n, int nrhs, double *a, long lda, int nb, int pivot_mode, int *ipiv)
@@ -889,18 +909,47 @@ static int lumcolumn_host(int n, double *a, double *b, int m, int *pv)
     const int nbw = gpu_panel_width(m);
     rc = check_matrix_args(n, 1, d, ld, nbw);
     if (rc) return rc;
+    // pinned (or registered) host matrix: finished factor blocks go back on a
+    // copy stream while the factorization continues; pageable memory would
+    // make those copies block the enqueuing thread, so it is copied at the end
+    cudaPointerAttributes pa{};
+    const bool pinned = cudaPointerGetAttributes(&pa, a) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    if (c->copy_stream) CU_TRY(cudaStreamSynchronize(c->copy_stream));  // nothing of an earlier call in flight
+    if (pinned && !c->copy_stream) {
+        CU_TRY(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+        CU_TRY(cudaEventCreateWithFlags(&c->copy_ev, cudaEventDisableTiming));
+    }
     if ((rc = begin_status(c))) return rc;
     CU_TRY(cudaMemcpy2DAsync(d, ld * sizeof(double), a, rdim * sizeof(double), (size_t)(n + 1) * sizeof(double), n,
                              cudaMemcpyHostToDevice, c->stream));
-    if ((rc = factor_enqueue(c, n, 1, d, ld, nbw, g_pivot_mode))) return rc;
+    const size_t pitch_h = rdim * sizeof(double), pitch_d = ld * sizeof(double);
+    auto copy_back = [&](int i, int w) -> int {
+        if (!pinned) return 0;
+        CU_TRY(cudaEventRecord(c->copy_ev, c->stream));
+        CU_TRY(cudaStreamWaitEvent(c->copy_stream, c->copy_ev, 0));
+        // rows i..i+w-1 from column i through column n (y), then columns i..i+w-1 of the rows below
+        CU_TRY(cudaMemcpy2DAsync(a + (size_t)i * rdim + i, pitch_h, d + (size_t)i * ld + i, pitch_d,
+                                 (size_t)(n + 1 - i) * sizeof(double), w, cudaMemcpyDeviceToHost, c->copy_stream));
+        if (i + w < n)
+            CU_TRY(cudaMemcpy2DAsync(a + (size_t)(i + w) * rdim + i, pitch_h, d + (size_t)(i + w) * ld + i, pitch_d,
+                                     (size_t)w * sizeof(double), n - i - w, cudaMemcpyDeviceToHost, c->copy_stream));
+        return 0;
+    };
+    if ((rc = factor_enqueue_with(c, n, 1, d, ld, nbw, g_pivot_mode, copy_back))) return rc;
     CU_TRY(cudaMemcpy2DAsync(x, sizeof(double), d + n, ld * sizeof(double), sizeof(double), n,
                              cudaMemcpyDeviceToDevice, c->stream));
     {
         PhaseTimer t(c, PH_BACKSOLVE);
         K_TRY(launch_backsolve(d, ld, n, 1, x, 1, c->stream));
     }
-    CU_TRY(cudaMemcpy2DAsync(a, rdim * sizeof(double), d, ld * sizeof(double), (size_t)(n + 1) * sizeof(double), n,
-                             cudaMemcpyDeviceToHost, c->stream));
+    if (pinned) {
+        CU_TRY(cudaEventRecord(c->copy_ev, c->copy_stream));
+        CU_TRY(cudaStreamWaitEvent(c->stream, c->copy_ev, 0));
+    } else {
+        CU_TRY(cudaMemcpy2DAsync(a, pitch_h, d, pitch_d, (size_t)(n + 1) * sizeof(double), n, cudaMemcpyDeviceToHost,
+                                 c->stream));
+    }
     CU_TRY(cudaMemcpyAsync(b, x, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     if (pv) {
         const int last = ((n - 1) / m) * m;

@@ -87,6 +87,29 @@ def test_lumcolumn_host_entry(oracle):
     assert np.abs(a[:, n] - ao[:, n]).max() / np.abs(ao[:, n]).max() < 1e-10
 
 
+@pytest.mark.parametrize("n,nb", [(1000, 256), (1500, 128), (37, 16)])
+def test_lumcolumn_pinned_host_overlaps_copies(oracle, n, nb):
+    """On pinned host buffers the finished factor blocks are copied back while
+    the factorization runs; the result is the same, bit for bit, as the one
+    copied back at the end for pageable buffers."""
+    import torch
+
+    a_pg = oracle.randomsetmat(n, 5)
+    b_pg = np.zeros(n)
+    pv_pg = np.zeros(nb, dtype=np.int32)
+    assert lumcolumn(a_pg, b_pg, nb, pv_pg, PIVOT_PARTIAL) == 0
+    a_t = torch.empty(a_pg.shape, dtype=torch.float64, pin_memory=True)
+    b_t = torch.zeros(n, dtype=torch.float64, pin_memory=True)
+    a_pin, b_pin = a_t.numpy(), b_t.numpy()
+    a_pin[...] = np.nan  # every element the factorization owns must be written back
+    a_pin[:, : n + 1] = oracle.randomsetmat(n, 5)[:, : n + 1]
+    pv_pin = np.zeros(nb, dtype=np.int32)
+    assert lumcolumn(a_pin, b_pin, nb, pv_pin, PIVOT_PARTIAL) == 0
+    np.testing.assert_array_equal(a_pin[:, : n + 1], a_pg[:, : n + 1])
+    np.testing.assert_array_equal(b_pin, b_pg)
+    np.testing.assert_array_equal(pv_pin, pv_pg)
+
+
 @pytest.mark.parametrize("n,nb", [(1, 16), (2, 16), (15, 16), (16, 16), (17, 16), (33, 16), (100, 32), (1000, 256),
                                   (777, 64)])
 def test_ragged_sizes_vs_lapack(ctx, oracle, n, nb):
