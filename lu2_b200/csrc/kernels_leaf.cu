@@ -12,13 +12,17 @@
 // Per column the critical path is one exchange between CTAs: every CTA
 // publishes its candidate (largest |a| among its rows, its row values, and --
 // from the CTA owning row c -- row c itself) in a slot stamped with a 64-bit
-// sequence number (release store); every CTA polls all slots (acquire loads),
-// reduces them to the same winner, fetches the winner's row and updates its
-// own rows.  Each thread owns fixed slab rows, so the exchange, the swap, the
-// rank-1 update and the next column's local argmax need only two CTA barriers
-// per column.  Slots are double-buffered by column parity: a CTA can be at
-// most one column ahead of any other, because it needs every CTA's previous
-// publication to advance.
+// sequence number (release store).  Warp 0 of every CTA waits for all slots
+// (each lane re-polls the slots it still waits for with back-to-back relaxed
+// loads, then one acquire fence), reduces them to the same winner, and after
+// a CTA barrier every warp fetches the winner's row and updates its own rows.
+// (Copying every candidate row into every CTA instead, which saves one L2 round
+// trip, measured slower: 148 CTAs reading the same 148 slot lines each column.)
+// Each thread owns fixed slab rows, so the exchange, the swap, the rank-1
+// update and the next column's local argmax need two CTA barriers per column.
+// Slots are double-buffered by column parity: a CTA can be at most one column
+// ahead of any other, because it needs every CTA's previous publication to
+// advance, and it reads a column's slots before its own next publication.
 #include <climits>
 
 #include "lu2gpu_internal.cuh"
@@ -63,14 +67,13 @@ __global__ void __launch_bounds__(LEAF_THREADS) leaf_kernel(LeafParams<T> P)
 {
     extern __shared__ __align__(16) unsigned char leaf_smem[];
     T *slab = reinterpret_cast<T *>(leaf_smem);
-    // per-warp partial argmax: [0] the CTA's own candidate, [1] the global one
-    // (separate arrays: warp 0 may still read [0] while others fill [1])
-    __shared__ double s_wv[2][LEAF_WARPS];
-    __shared__ int s_wi[2][LEAF_WARPS];
-    __shared__ int s_fail;
     const int G = gridDim.x, bid = blockIdx.x, tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
     const int w = P.w, c0 = P.c0, rpc = P.rows_per_cta;
+    // per-warp partial argmax of the CTA's own candidate; the column's winner
+    __shared__ double s_wv[LEAF_WARPS];
+    __shared__ int s_wi[LEAF_WARPS];
+    __shared__ int s_fail, s_win;
     const int rb = c0 + bid * rpc;
     const int re = min(P.n, rb + rpc);
     const int nr = max(0, re - rb);
@@ -115,13 +118,13 @@ __global__ void __launch_bounds__(LEAF_THREADS) leaf_kernel(LeafParams<T> P)
         // CTA candidate -> warp 0 publishes it (and row c, from its owner)
         warp_argmax(bv, bi);
         if (lane == 0) {
-            s_wv[0][warp] = bv;
-            s_wi[0][warp] = bi;
+            s_wv[warp] = bv;
+            s_wi[warp] = bi;
         }
         __syncthreads();  // S1
         if (warp == 0) {
-            double v = lane < LEAF_WARPS ? s_wv[0][lane] : -1.0;
-            int i = lane < LEAF_WARPS ? s_wi[0][lane] : INT_MAX;
+            double v = lane < LEAF_WARPS ? s_wv[lane] : -1.0;
+            int i = lane < LEAF_WARPS ? s_wi[lane] : INT_MAX;
             warp_argmax(v, i);
             if (lane < LEAF_W) {
                 myslot->row[lane] = (i != INT_MAX) ? slab[(i - rb) * LEAF_LDS + lane] : 0.0;
@@ -136,22 +139,32 @@ __global__ void __launch_bounds__(LEAF_THREADS) leaf_kernel(LeafParams<T> P)
             if (lane == 0) st_release_u64(&myslot->seq, seq);
         }
 
-        // warp 0 waits for every CTA's candidate of this column (relaxed polls,
-        // then one acquire fence) and reduces them to the winner
+        // warp 0 waits for every CTA's candidate of this column and reduces
+        // them to the winner.  Each lane watches up to LEAF_THREADS/32 slots:
+        // it loads all those it still waits for back to back (relaxed), so the
+        // polls overlap instead of costing one L2 round trip each; then one
+        // acquire fence per lane before the candidates are read.
         if (warp == 0) {
-            double gv = -1.0;
-            int gi = INT_MAX;
+            constexpr int QMAX = LEAF_THREADS / 32;
+            const LeafSlot *sl = P.slots + (size_t)par * G;
+            unsigned pending = 0;
+#pragma unroll
+            for (int k = 0; k < QMAX; k++)
+                if (lane + 32 * k < G) pending |= 1u << k;
             const unsigned long long t0 = globaltimer_ns();
+            unsigned spins = 0;
             bool failed = false;
-            for (int q = lane; q < G && !failed; q += 32) {
-                const unsigned long long *sq = &P.slots[(size_t)par * G + q].seq;
-                unsigned spins = 0;
-                while (ld_relaxed_u64(sq) != seq) {
-                    if ((++spins & 255u) == 0 &&
-                        (*(volatile int *)&P.status[1] != 0 || globaltimer_ns() - t0 > WAIT_LIMIT_NS)) {
-                        failed = true;
-                        break;
-                    }
+            while (pending) {
+                unsigned long long sv[QMAX];
+#pragma unroll
+                for (int k = 0; k < QMAX; k++) sv[k] = ((pending >> k) & 1u) ? ld_relaxed_u64(&sl[lane + 32 * k].seq) : 0ull;
+#pragma unroll
+                for (int k = 0; k < QMAX; k++)
+                    if (((pending >> k) & 1u) && sv[k] == seq) pending &= ~(1u << k);
+                if (pending && (++spins & 63u) == 0 &&
+                    (*(volatile int *)&P.status[1] != 0 || globaltimer_ns() - t0 > WAIT_LIMIT_NS)) {
+                    failed = true;
+                    break;
                 }
             }
             if (__any_sync(0xffffffffu, failed)) {
@@ -161,34 +174,32 @@ __global__ void __launch_bounds__(LEAF_THREADS) leaf_kernel(LeafParams<T> P)
                 }
             } else {
                 asm volatile("fence.acq_rel.gpu;" ::: "memory");  // acquire side of the slots' release stores
+                double gv = -1.0;
+                int gi = INT_MAX;
                 for (int q = lane; q < G; q += 32) {
-                    const LeafSlot *s = P.slots + (size_t)par * G + q;
-                    const double v = __ldcg(&s->val);
-                    const int i = __ldcg(&s->idx);
+                    const double v = __ldcg(&sl[q].val);
+                    const int i = __ldcg(&sl[q].idx);
                     if (argmax_better(v, i, gv, gi)) {
                         gv = v;
                         gi = i;
                     }
                 }
                 warp_argmax(gv, gi);
-                if (lane == 0) {
-                    s_wv[1][0] = gv;
-                    s_wi[1][0] = gi;
-                }
+                if (lane == 0) s_win = gi;
             }
         }
         __syncthreads();  // S2
         if (s_fail) break;
-        const double gv = s_wv[1][0];
-        const int gi = s_wi[1][0];
-        (void)gv;
+        const int gi = s_win;
 
         const int p = (gi == INT_MAX) ? c : gi;  // no finite candidate (a NaN column): keep row c
         const int owner_p = (p - c0) / rpc, owner_c = (c - c0) / rpc;
-        // lanes 0..15: the pivot row; lanes 16..31: old row c
+        // lanes 0..15: the pivot row (row c itself when there is no finite
+        // candidate); lanes 16..31: old row c
         double pr = 0.0;
         if (lane < LEAF_W && lane < w)
-            pr = __ldcg(&P.slots[(size_t)par * G + owner_p].row[lane]);
+            pr = (gi == INT_MAX) ? __ldcg(&P.slots[(size_t)par * G + owner_c].rowc[lane])
+                                 : __ldcg(&P.slots[(size_t)par * G + owner_p].row[lane]);
         else if (lane >= LEAF_W && lane - LEAF_W < w)
             pr = __ldcg(&P.slots[(size_t)par * G + owner_c].rowc[lane - LEAF_W]);
         const T d = (T)__shfl_sync(0xffffffffu, pr, ip);
