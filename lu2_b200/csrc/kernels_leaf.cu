@@ -258,6 +258,11 @@ __global__ void __launch_bounds__(LEAF_THREADS) leaf_kernel(LeafParams<T> P)
     }
 }
 
+int leaf_min_ctas(int rows, size_t tsize)
+{
+    return (int)(((size_t)rows * LEAF_LDS * tsize + LEAF_SMEM_MAX - 1) / LEAF_SMEM_MAX);
+}
+
 int leaf_max_ctas(int device)
 {
     int sms = 0, per_sm = 0;

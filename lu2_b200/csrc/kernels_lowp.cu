@@ -397,7 +397,8 @@ static cudaError_t lp_map(CUtensorMap *m, CUtensorMapDataType dt, int esize, con
 
 template <bool FP8>
 static cudaError_t lp_launch(const void *a, long lda, const void *bt, long ldb, float *c, long ldc, int M, int N,
-                             int K, const float *scale, const float *da, const float *db, int *status, cudaStream_t st)
+                             int K, const float *scale, const float *da, const float *db, int *status, int max_ctas,
+                             cudaStream_t st)
 {
     if (M <= 0 || N <= 0) return cudaSuccess;
     const int chunk = FP8 ? 128 : 64;
@@ -429,6 +430,7 @@ static cudaError_t lp_launch(const void *a, long lda, const void *bt, long ldb, 
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
     const long tiles = (long)p.tiles_m * p.tiles_n;
     if (tiles > 0x7fffffffL) return cudaErrorInvalidConfiguration;
+    if (max_ctas > 0 && max_ctas < sms) sms = max_ctas;  // leave SMs to a concurrent panel
     const int grid = tiles < sms ? (int)tiles : sms;
     count_launch();
     lowp_update_kernel<FP8><<<grid, LP_THREADS, LP_SMEM, st>>>(ta, tb, tc, p);
@@ -436,16 +438,16 @@ static cudaError_t lp_launch(const void *a, long lda, const void *bt, long ldb, 
 }
 
 cudaError_t launch_lowp_update_bf16(const void *a16, long lda, const void *bt16, long ldb, float *c, long ldc, int M,
-                                    int N, int K, const float *scale, int *status, cudaStream_t st)
+                                    int N, int K, const float *scale, int *status, int max_ctas, cudaStream_t st)
 {
-    return lp_launch<false>(a16, lda, bt16, ldb, c, ldc, M, N, K, scale, nullptr, nullptr, status, st);
+    return lp_launch<false>(a16, lda, bt16, ldb, c, ldc, M, N, K, scale, nullptr, nullptr, status, max_ctas, st);
 }
 
 cudaError_t launch_lowp_update_fp8(const uint8_t *a8, long lda, const float *da, const uint8_t *bt8, long ldb,
                                    const float *db, float *c, long ldc, int M, int N, int K, int *status,
-                                   cudaStream_t st)
+                                   int max_ctas, cudaStream_t st)
 {
-    return lp_launch<true>(a8, lda, bt8, ldb, c, ldc, M, N, K, nullptr, da, db, status, st);
+    return lp_launch<true>(a8, lda, bt8, ldb, c, ldc, M, N, K, nullptr, da, db, status, max_ctas, st);
 }
 
 }  // namespace lu2gpu

@@ -1398,6 +1398,9 @@ struct MixedWork {
     size_t bt32top_cap = 0;
     double *gm = nullptr;  // GMRES: basis (restart+1 vectors), w, z, d, t, partial sums, dots
     size_t gm_cap = 0;
+    // lookahead: panel k+1 on `side` while the rest of update k runs on the context's stream
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_cols = nullptr, ev_panel = nullptr;
 };
 
 static void free_mixed(lu2gpu_ctx *c)
@@ -1416,6 +1419,12 @@ static void free_mixed(lu2gpu_ctx *c)
     cudaFree(m->dq);
     cudaFree(m->bt32top);
     cudaFree(m->gm);
+    if (m->side) {
+        cudaStreamSynchronize(m->side);
+        cudaStreamDestroy(m->side);
+    }
+    if (m->ev_cols) cudaEventDestroy(m->ev_cols);
+    if (m->ev_panel) cudaEventDestroy(m->ev_panel);
     delete m;
     c->mx = nullptr;
 }
@@ -1453,9 +1462,17 @@ struct View32 {
     int n, ncols, goff;
 };
 
+// Top-level right part of the precision forms with the trailing update in two
+// launches: columns cs..cs+w1-1 first (the next panel's), then `after_first()`
+// (the lookahead hook), then the rest; update kernels capped at max_ctas CTAs.
+template <typename Hook>
+static int right_part32_split(lu2gpu_ctx *c, const View32 &v, int k0, int k1, int cs, int ce, int w1, int max_ctas,
+                              Hook after_first);
+
 static int right_part32(lu2gpu_ctx *c, const View32 &v, int k0, int k1, int cs, int ce, bool top)
 {
     if (ce <= cs) return 0;
+    if (top) return right_part32_split(c, v, k0, k1, cs, ce, 0, 0, []() { return 0; });
     MixedWork *m = c->mx;
     int *ipiv = c->d_ipiv + v.goff;
     float *dinv = m->dinv + v.goff;
@@ -1472,42 +1489,78 @@ static int right_part32(lu2gpu_ctx *c, const View32 &v, int k0, int k1, int cs, 
         if (k1 < v.n)
             K_TRY(launch_sgemm_update(v.a + (size_t)k1 * v.ld + k0, v.ld, m->bt32, v.a + (size_t)k1 * v.ld + cs, v.ld,
                                       v.n - k1, ce - cs, K, c->stream));
-        return 0;
     }
+    return 0;
+}
+
+template <typename Hook>
+static int right_part32_split(lu2gpu_ctx *c, const View32 &v, int k0, int k1, int cs, int ce, int w1, int max_ctas,
+                              Hook after_first)
+{
+    if (ce <= cs) return after_first();
+    MixedWork *m = c->mx;
+    int *ipiv = c->d_ipiv + v.goff;
+    float *dinv = m->dinv + v.goff;
+    const int K = k1 - k0, M = v.n - k1, N = ce - cs;
+    // the second launch starts at a quantization tile boundary of U12^T
+    if (w1 <= 0 || w1 >= N || (w1 % 128)) w1 = N;
+    {
+        PhaseTimer t(c, PH_SWAP);
+        K_TRY(launch_laswp_scale(v.a, v.ld, k0, k1, ipiv, v.goff, dinv, cs, ce, true, c->stream));
+    }
+    const float *T = v.a + (size_t)k0 * v.ld + k0;
+    float *X = v.a + (size_t)k0 * v.ld + cs;
+    const float *L = v.a + (size_t)k1 * v.ld + k0;
+    float *C = v.a + (size_t)k1 * v.ld + cs;
+    int rc;
     if (m->update == LU2GPU_UPDATE_FP8) {
-        const int M = v.n - k1, N = ce - cs;
         {
             PhaseTimer t(c, PH_TRSM);
             // U12 solved in place; its transpose (N x K, FP32) feeds the quantizer
             K_TRY(launch_trsm_unit_lower_f32(T, v.ld, X, v.ld, K, N, k1 < v.n ? m->bt32top : nullptr, c->stream));
         }
-        if (k1 < v.n) {
+        if (k1 >= v.n) return after_first();
+        const int KB = K / 128;
+        float *dqa = m->dq, *dqb = m->dq + (((size_t)M + 127) / 128) * KB;
+        {
             PhaseTimer t(c, PH_DGEMM);
-            const float *L = v.a + (size_t)k1 * v.ld + k0;
-            float *dqa = m->dq, *dqb = m->dq + (((size_t)M + 127) / 128) * (K / 128);
             K_TRY(launch_quant_fp8_tiles(L, v.ld, M, K, m->l8, K, dqa, c->stream));
             K_TRY(launch_quant_fp8_tiles(m->bt32top, K, N, K, m->b8, K, dqb, c->stream));
-            K_TRY(launch_lowp_update_fp8(m->l8, K, dqa, m->b8, K, dqb, v.a + (size_t)k1 * v.ld + cs, v.ld, M, N, K,
-                                         c->d_status, c->stream));
+            K_TRY(launch_lowp_update_fp8(m->l8, K, dqa, m->b8, K, dqb, C, v.ld, M, w1, K, c->d_status, max_ctas,
+                                         c->stream));
+        }
+        rc = after_first();
+    if (rc) return rc;
+        if (w1 < N) {
+            PhaseTimer t(c, PH_DGEMM);
+            K_TRY(launch_lowp_update_fp8(m->l8, K, dqa, m->b8 + (size_t)w1 * K, K, dqb + (size_t)(w1 / 128) * KB,
+                                         C + w1, v.ld, M, N - w1, K, c->d_status, max_ctas, c->stream));
         }
         return 0;
     }
     {
         PhaseTimer t(c, PH_TRSM);
-        K_TRY(launch_trsm_unit_lower_f32(T, v.ld, X, v.ld, K, ce - cs, nullptr, c->stream));
+        K_TRY(launch_trsm_unit_lower_f32(T, v.ld, X, v.ld, K, N, nullptr, c->stream));
     }
-    if (k1 < v.n) {
+    if (k1 >= v.n) return after_first();
+    const char *u16 = static_cast<const char *>(m->u16);
+    {
         PhaseTimer t(c, PH_DGEMM);
-        const int M = v.n - k1, N = ce - cs;
-        const float *L = v.a + (size_t)k1 * v.ld + k0;
         CU_TRY(cudaMemsetAsync(m->amax(), 0, 2 * sizeof(unsigned), c->stream));
         K_TRY(launch_absmax(L, v.ld, M, K, m->amax(), c->stream));
         K_TRY(launch_absmax(X, v.ld, K, N, m->amax() + 1, c->stream));
         K_TRY(launch_panel_scales(m->amax(), m->scales(), c->stream));
         K_TRY(launch_f32_to_bf16(L, v.ld, m->l16, K, M, K, m->scales(), c->stream));
         K_TRY(launch_f32_transpose_bf16(X, v.ld, K, N, m->u16, m->scales() + 1, c->stream));
-        K_TRY(launch_lowp_update_bf16(m->l16, K, m->u16, K, v.a + (size_t)k1 * v.ld + cs, v.ld, M, N, K,
-                                      m->scales() + 2, c->d_status, c->stream));
+        K_TRY(launch_lowp_update_bf16(m->l16, K, u16, K, C, v.ld, M, w1, K, m->scales() + 2, c->d_status, max_ctas,
+                                      c->stream));
+    }
+    rc = after_first();
+    if (rc) return rc;
+    if (w1 < N) {
+        PhaseTimer t(c, PH_DGEMM);
+        K_TRY(launch_lowp_update_bf16(m->l16, K, u16 + (size_t)w1 * K * 2, K, C + w1, v.ld, M, N - w1, K,
+                                      m->scales() + 2, c->d_status, max_ctas, c->stream));
     }
     return 0;
 }
@@ -1562,7 +1615,7 @@ extern "C" int lu2gpu_bf16_update_dev(lu2gpu_ctx *c, int M, int N, int K, const 
     // the scale travels as a device scalar (the factorization computes it on the device)
     float *dscale = reinterpret_cast<float *>(c->d_bt);
     CU_TRY(cudaMemcpyAsync(dscale, &scale, sizeof(float), cudaMemcpyHostToDevice, c->stream));
-    K_TRY(launch_lowp_update_bf16(a16, lda, bt16, ldb, c32, ldc, M, N, K, dscale, c->d_status, c->stream));
+    K_TRY(launch_lowp_update_bf16(a16, lda, bt16, ldb, c32, ldc, M, N, K, dscale, c->d_status, 0, c->stream));
     return end_status(c, "lu2gpu_bf16_update_dev");
 }
 
@@ -2000,9 +2053,8 @@ extern "C" int lu2gpu_batch_sizes(int count, long seed, int nmin, int nmax, doub
 }
 
 // lumcolumn's panel loop (lu2.c:1126-1141) on the FP32 working matrix
-static int factor32_or_fail(lu2gpu_ctx *c, int n, float *a, long ld, int nb, int mode)
+static int factor32_serial(lu2gpu_ctx *c, const View32 &v, int n, int nb, int mode)
 {
-    View32 v{a, ld, n, n, 0};
     for (int i = 0; i < n; i += nb) {
         const int w = (n - i) < nb ? (n - i) : nb;
         int rc = panel32(c, v, i, w, mode);
@@ -2010,6 +2062,69 @@ static int factor32_or_fail(lu2gpu_ctx *c, int n, float *a, long ld, int nb, int
         if ((rc = right_part32(c, v, i, i + w, i + w, n, true))) return rc;
     }
     return 0;
+}
+
+// Lookahead (the reference's lu_mpi_blocked_lookahead idea, lu2_mpi.c:3643-
+// 3847, on one GPU): step k updates the next panel's columns first, then the
+// next panel is factored on a second stream while the rest of the update runs.
+// The persistent update kernel is held to sms - R CTAs (one per SM, by its
+// shared memory), which leaves R SMs for the panel's leaf CTAs (R = the
+// fewest CTAs whose FP32 slab fits, at least 24).  Step k+1's right part waits
+// for that panel: its row exchanges cross the columns the update wrote.
+// Serial when phase timing is on (so the phase split stays meaningful), for
+// small n, or with LU2GPU_LOOKAHEAD=0.
+static int factor32_or_fail(lu2gpu_ctx *c, int n, float *a, long ld, int nb, int mode)
+{
+    View32 v{a, ld, n, n, 0};
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+    const int R = std::max(24, leaf_min_ctas(n, sizeof(float)));
+    const char *env = getenv("LU2GPU_LOOKAHEAD");
+    const bool lookahead = !c->timing && n >= 4 * nb && 2 * R < sms && !(env && env[0] == '0');
+    if (!lookahead) return factor32_serial(c, v, n, nb, mode);
+    MixedWork *m = c->mx;
+    if (!m->side) {
+        CU_TRY(cudaStreamCreateWithFlags(&m->side, cudaStreamNonBlocking));
+        CU_TRY(cudaEventCreateWithFlags(&m->ev_cols, cudaEventDisableTiming));
+        CU_TRY(cudaEventCreateWithFlags(&m->ev_panel, cudaEventDisableTiming));
+    }
+    const cudaStream_t main_st = c->stream;
+    const int all_ctas = c->leaf_ctas;
+    int rc = panel32(c, v, 0, std::min(nb, n), mode);  // the first panel, on the main stream
+    for (int i = 0; rc == 0 && i < n; i += nb) {
+        const int w = std::min(nb, n - i), i1 = i + w, w1 = std::min(nb, n - i1);
+        if (i > 0 && cudaStreamWaitEvent(main_st, m->ev_panel, 0) != cudaSuccess) {
+            set_error("lookahead: cudaStreamWaitEvent failed");
+            rc = LU2GPU_ERR_CUDA;
+            break;
+        }
+        auto next_panel = [&]() -> int {
+            if (i1 >= n) return 0;
+            CU_TRY(cudaEventRecord(m->ev_cols, main_st));
+            CU_TRY(cudaStreamWaitEvent(m->side, m->ev_cols, 0));
+            c->stream = m->side;
+            c->leaf_ctas = std::min(all_ctas, R);
+            const int r = panel32(c, v, i1, w1, mode);
+            c->stream = main_st;
+            c->leaf_ctas = all_ctas;
+            if (r) return r;
+            CU_TRY(cudaEventRecord(m->ev_panel, m->side));
+            return 0;
+        };
+        rc = right_part32_split(c, v, i, i1, i1, n, w1, sms - R, next_panel);
+    }
+    c->stream = main_st;
+    c->leaf_ctas = all_ctas;
+    // everything on the side stream precedes what follows on the main stream
+    if (cudaEventRecord(m->ev_panel, m->side) != cudaSuccess ||
+        cudaStreamWaitEvent(main_st, m->ev_panel, 0) != cudaSuccess) {
+        cudaGetLastError();
+        if (!rc) {
+            set_error("lookahead: joining the panel stream failed");
+            rc = LU2GPU_ERR_CUDA;
+        }
+    }
+    return rc;
 }
 
 extern "C" int lu2gpu_mixed_solve(lu2gpu_ctx *c, int n, const double *a, long lda, const double *b, double *x, int nb,
@@ -2324,6 +2439,6 @@ extern "C" int lu2gpu_fp8_update_dev(lu2gpu_ctx *c, int M, int N, int K, const f
     K_TRY(launch_quant_fp8_tiles(bt, ldb, N, K, b8, K, dqb, c->stream));
     if (a_deq) K_TRY(launch_dequant_fp8_tiles(a8, K, dqa, M, K, a_deq, K, c->stream));
     if (bt_deq) K_TRY(launch_dequant_fp8_tiles(b8, K, dqb, N, K, bt_deq, K, c->stream));
-    K_TRY(launch_lowp_update_fp8(a8, K, dqa, b8, K, dqb, c32, ldc, M, N, K, c->d_status, c->stream));
+    K_TRY(launch_lowp_update_fp8(a8, K, dqa, b8, K, dqb, c32, ldc, M, N, K, c->d_status, 0, c->stream));
     return end_status(c, "lu2gpu_fp8_update_dev");
 }

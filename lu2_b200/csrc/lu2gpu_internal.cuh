@@ -93,6 +93,8 @@ cudaError_t launch_leaf(double *a, long ld, int n, int c0, int w, int mode, int 
 cudaError_t launch_leaf(float *a, long ld, int n, int c0, int w, int mode, int goff, int *ipiv, float *dinv,
                         const LeafBuffers &buf, int *status, int max_ctas, cudaStream_t st);
 int leaf_max_ctas(int device);
+// fewest leaf CTAs whose slabs of `rows` rows (elements of tsize bytes) fit shared memory
+int leaf_min_ctas(int rows, size_t tsize);
 
 // Apply the pivots k0..k1-1 (row k <-> row ipiv[k], in order) to columns
 // cs..ce-1 and, when `scale`, multiply row k by dinv[k] after its swap.
@@ -217,11 +219,12 @@ cudaError_t launch_vec_absmax(const double *v, int n, unsigned long long *out, c
 // (kernels_lowp.cu): C (FP32, 16-byte aligned, ldc a multiple of 4) -=
 // *scale * A Bt^T with BF16 operands (K a multiple of 64, <= 256), or
 // -= sum_kb da db Aq_kb Bq_kb^T with E4M3 operands and per-tile scales (K = 128 or 256)
+// (max_ctas > 0 caps the persistent grid, leaving SMs free for a concurrent panel)
 cudaError_t launch_lowp_update_bf16(const void *a16, long lda, const void *bt16, long ldb, float *c, long ldc, int M,
-                                    int N, int K, const float *scale, int *status, cudaStream_t st);
+                                    int N, int K, const float *scale, int *status, int max_ctas, cudaStream_t st);
 cudaError_t launch_lowp_update_fp8(const uint8_t *a8, long lda, const float *da, const uint8_t *bt8, long ldb,
                                    const float *db, float *c, long ldc, int M, int N, int K, int *status,
-                                   cudaStream_t st);
+                                   int max_ctas, cudaStream_t st);
 
 // FP8 form operands (kernels_fp8.cu): per-128x128-tile E4M3 quantization with power-of-two scales; dq = [ceil(rows/128)][cols/128]
 cudaError_t launch_quant_fp8_tiles(const float *x, long ldx, int rows, int cols, uint8_t *q, long ldq, float *dq,
