@@ -69,3 +69,28 @@ def test_mixed_solve_rejects_bad_block(ctx):
     x = torch.zeros(n, dtype=torch.float64, device="cuda")
     with pytest.raises(L.Lu2GpuError):
         ctx.mixed_solve(a, n, ld, b, x, 48)
+
+
+@pytest.mark.parametrize("update", ["bf16", "fp8"])
+def test_lookahead_matches_serial_factorization(ctx, monkeypatch, update):
+    """The lookahead schedule (next panel on a second stream beside the capped
+    update) computes exactly what the serial one does: same tiles, same per-row
+    arithmetic in the leaf, only the order of independent work changes."""
+    import torch
+
+    n, nb = 3000, 256
+    a, ld, b = _dd_system(ctx, n, 29)
+    xs = []
+    for env in ("0", None):
+        if env is None:
+            monkeypatch.delenv("LU2GPU_LOOKAHEAD", raising=False)
+        else:
+            monkeypatch.setenv("LU2GPU_LOOKAHEAD", env)
+        x = torch.zeros(n, dtype=torch.float64, device="cuda")
+        if update == "bf16":
+            res = ctx.mixed_solve(a, n, ld, b, x, nb)
+        else:
+            res = ctx.gmres_solve(a, n, ld, b, x, nb, update=L.UPDATE_FP8)
+        assert res["status"] == 0, res
+        xs.append(x)
+    assert torch.equal(xs[0], xs[1])
