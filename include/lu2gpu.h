@@ -265,7 +265,8 @@ int lu2gpu_batch_restore(lu2gpu_batch *b);
 int lu2gpu_batch_set_mode(lu2gpu_batch *b, int mode, int max_iter);
 /* Corrections each system took in the last FP32_IR solve (count ints). */
 int lu2gpu_batch_iterations(lu2gpu_batch *b, int *iters_host);
-/* Launch shape: threads per CTA, panel width of the blocked path, CTAs per SM. */
+/* Launch shape: threads per CTA (64..512, a multiple of 32), panel width of
+ * the blocked path (16..64), CTAs per SM. */
 int lu2gpu_batch_set_config(lu2gpu_batch *b, int threads, int pw, int ctas_per_sm);
 /* Time the launch shapes on this batch and keep the fastest; params_out (4
  * ints, may be NULL) = {threads, panel width, CTAs per SM, microseconds}. */

@@ -12,8 +12,8 @@
 // a host-sorted order).  A system whose augmented matrix fits the shared
 // memory budget is factored and solved there; larger ones run a blocked LU on
 // the L2-resident matrix with the panel (all remaining rows x pw columns) in
-// shared memory and the trailing update computed from a shared-memory copy of
-// the U block in 4 x 4 register tiles.
+// shared memory and the trailing update on the FP64 tensor cores (mma.sync
+// m16n8k8) from the panel and a shared-memory copy of the U block.
 #include <climits>
 
 #include "lu2gpu_internal.cuh"
@@ -94,25 +94,38 @@ __device__ void batch_solve_smem(double *A, long ld, int n, int nrhs, double *S,
     if (tid == 0) *info = first_zero;
 }
 
+__device__ __forceinline__ void batch_dmma(double (&c)[4], double a0, double a1, double a2, double a3, double b0,
+                                           double b1)
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+        : "d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(b0), "d"(b1));
+}
+
 // blocked LU in global memory (L2-resident), panel of pw columns in shared memory
 __device__ void batch_solve_blocked(double *A, long ld, int n, int nrhs, int pw, double *P, double *U, int *piv,
                                     double *dinv, int *info, double *s_v, int *s_i)
 {
     const int nc = n + nrhs, T = blockDim.x, tid = threadIdx.x;
+    // panel row stride: the 8 rows a warp's MMA fragment load touches fall
+    // into different banks (2 * (pw + 4) doubles = 8 banks apart for pw % 16 == 0)
+    const int ps = pw + BATCH_PANEL_PAD;
     int first_zero = 0;
     for (int k0 = 0; k0 < n; k0 += pw) {
         const int w = min(pw, n - k0), rows = n - k0;
-        // panel rows k0..n-1, columns k0..k0+w-1 -> P (rows x pw)
+        // panel rows k0..n-1, columns k0..k0+w-1 -> P (rows x ps)
         for (int idx = tid; idx < rows * w; idx += T) {
             const int r = idx / w, c = idx - r * w;
-            P[r * pw + c] = A[(size_t)(k0 + r) * ld + k0 + c];
+            P[r * ps + c] = A[(size_t)(k0 + r) * ld + k0 + c];
         }
         __syncthreads();
         for (int c = 0; c < w; c++) {
             double v = -1.0;
             int p = INT_MAX;
             for (int r = c + tid; r < rows; r += T) {
-                const double a = fabs(P[r * pw + c]);
+                const double a = fabs(P[r * ps + c]);
                 if (a > v) {
                     v = a;
                     p = r;
@@ -123,32 +136,32 @@ __device__ void batch_solve_blocked(double *A, long ld, int n, int nrhs, int pw,
             if (tid == 0) piv[c] = p;
             if (p != c)
                 for (int j = tid; j < w; j += T) {
-                    const double t = P[c * pw + j];
-                    P[c * pw + j] = P[p * pw + j];
-                    P[p * pw + j] = t;
+                    const double t = P[c * ps + j];
+                    P[c * ps + j] = P[p * ps + j];
+                    P[p * ps + j] = t;
                 }
             __syncthreads();
-            const double d = P[c * pw + c];
+            const double d = P[c * ps + c];
             const bool zero = (d == 0.0);
             if (zero && !first_zero) first_zero = k0 + c + 1;
             const double inv = zero ? 1.0 : 1.0 / d;
             if (tid == 0) dinv[c] = inv;
             if (!zero)
                 for (int j = tid; j < w; j += T)
-                    if (j != c) P[c * pw + j] *= inv;
+                    if (j != c) P[c * ps + j] *= inv;
             __syncthreads();
             if (!zero) {
                 const int wj = w - c - 1, hr = rows - c - 1;
                 for (int idx = tid; idx < hr * wj; idx += T) {
                     const int r = c + 1 + idx / wj, j = c + 1 + idx % wj;
-                    P[r * pw + j] -= P[r * pw + c] * P[c * pw + j];
+                    P[r * ps + j] -= P[r * ps + c] * P[c * ps + j];
                 }
             }
             __syncthreads();
         }
         for (int idx = tid; idx < rows * w; idx += T) {
             const int r = idx / w, c = idx - r * w;
-            A[(size_t)(k0 + r) * ld + k0 + c] = P[r * pw + c];
+            A[(size_t)(k0 + r) * ld + k0 + c] = P[r * ps + c];
         }
         __syncthreads();
         // right part: exchanges with 1/pivot scaling, then the unit-lower solve
@@ -170,43 +183,84 @@ __device__ void batch_solve_blocked(double *A, long ld, int n, int nrhs, int pw,
             }
             for (int r = 1; r < w; r++) {
                 double s = x[r];
-                for (int l = 0; l < r; l++) s -= P[r * pw + l] * x[l];
+                for (int l = 0; l < r; l++) s -= P[r * ps + l] * x[l];
                 x[r] = s;
             }
             for (int c = 0; c < w; c++) A[(size_t)(k0 + c) * ld + j] = x[c];
         }
         __syncthreads();
-        // trailing update A[k0+w.., cs..] -= L21 U12 in 64-column chunks
+        // trailing update A[k0+w.., cs..] -= L21 U12 on the FP64 tensor cores
+        // (mma.sync m16n8k8 f64), in 64-column chunks of U12 staged in shared
+        // memory; a warp takes 16 x 32 units (two per chunk row strip): C
+        // fragments from global memory, -L21 fragments from the panel, U12
+        // fragments from the chunk, K padded to a multiple of 8 with zeros
         const int h = n - cs;
+        const int warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3, nwarps = T >> 5;
+        const int ksteps = (w + 7) >> 3;
+        const bool even = (cs & 1) == 0;  // 16-byte C accesses need an even column (always so: w = pw here)
         for (int c0 = cs; c0 < nc && h > 0; c0 += 64) {
             const int cw = min(64, nc - c0);
-            for (int idx = tid; idx < w * 64; idx += T) {
+            for (int idx = tid; idx < pw * 64; idx += T) {
                 const int l = idx >> 6, c = idx & 63;
-                U[l * 64 + c] = (c < cw) ? A[(size_t)(k0 + l) * ld + c0 + c] : 0.0;
+                U[l * BATCH_U_STRIDE + c] = (l < w && c < cw) ? A[(size_t)(k0 + l) * ld + c0 + c] : 0.0;
             }
             __syncthreads();
-            const int tx = tid & 15, ty = tid >> 4, tys = T >> 4;
-            for (int rb = ty * 4; rb < h; rb += tys * 4) {
-                double acc[4][4] = {};
-                for (int l = 0; l < w; l++) {
-                    double av[4], bv[4];
+            const int units = ((h + 15) >> 4) * 2;
+            for (int u = warp; u < units; u += nwarps) {
+                const int r0 = (u >> 1) << 4, cb = (u & 1) << 5;  // strip rows r0.., chunk columns cb..cb+31
+                const int rl = r0 + g, rh = rl + 8;                // rows (of the trailing block) of c0,c1 / c2,c3
+                double acc[4][4];
 #pragma unroll
-                    for (int i = 0; i < 4; i++) {
-                        av[i] = (rb + i < h) ? P[(w + rb + i) * pw + l] : 0.0;
-                        bv[i] = U[l * 64 + tx * 4 + i];
+                for (int j = 0; j < 4; j++) {
+                    const int col = cb + 8 * j + 2 * t;  // chunk column of c0 / c2
+#pragma unroll
+                    for (int hh = 0; hh < 2; hh++) {
+                        const int r = hh ? rh : rl;
+                        double v0 = 0.0, v1 = 0.0;
+                        if (r < h && col < cw) {
+                            const double *cp = A + (size_t)(cs + r) * ld + c0 + col;
+                            if (even && col + 1 < cw) {
+                                const double2 v = *reinterpret_cast<const double2 *>(cp);
+                                v0 = v.x;
+                                v1 = v.y;
+                            } else {
+                                v0 = cp[0];
+                                if (col + 1 < cw) v1 = cp[1];
+                            }
+                        }
+                        acc[j][2 * hh] = v0;
+                        acc[j][2 * hh + 1] = v1;
                     }
+                }
+                for (int kk = 0; kk < ksteps; kk++) {
+                    const int ka = 8 * kk + t, kb = ka + 4;
+                    const double *pl = P + (size_t)(w + rl) * ps, *ph = P + (size_t)(w + rh) * ps;
+                    const double a0 = (rl < h && ka < w) ? -pl[ka] : 0.0;
+                    const double a1 = (rh < h && ka < w) ? -ph[ka] : 0.0;
+                    const double a2 = (rl < h && kb < w) ? -pl[kb] : 0.0;
+                    const double a3 = (rh < h && kb < w) ? -ph[kb] : 0.0;
 #pragma unroll
-                    for (int i = 0; i < 4; i++)
-#pragma unroll
-                        for (int q = 0; q < 4; q++) acc[i][q] = fma(av[i], bv[q], acc[i][q]);
+                    for (int j = 0; j < 4; j++) {
+                        const double b0 = U[ka * BATCH_U_STRIDE + cb + 8 * j + g];
+                        const double b1 = U[kb * BATCH_U_STRIDE + cb + 8 * j + g];
+                        batch_dmma(acc[j], a0, a1, a2, a3, b0, b1);
+                    }
                 }
 #pragma unroll
-                for (int i = 0; i < 4; i++) {
-                    if (rb + i >= h) break;
-                    double *row = A + (size_t)(cs + rb + i) * ld + c0;
+                for (int j = 0; j < 4; j++) {
+                    const int col = cb + 8 * j + 2 * t;
 #pragma unroll
-                    for (int q = 0; q < 4; q++)
-                        if (tx * 4 + q < cw) row[tx * 4 + q] -= acc[i][q];
+                    for (int hh = 0; hh < 2; hh++) {
+                        const int r = hh ? rh : rl;
+                        if (r >= h || col >= cw) continue;
+                        double *cp = A + (size_t)(cs + r) * ld + c0 + col;
+                        if (even && col + 1 < cw) {
+                            *reinterpret_cast<double2 *>(cp) = make_double2(acc[j][2 * hh], acc[j][2 * hh + 1]);
+                        } else {
+                            cp[0] = acc[j][2 * hh];
+                            if (col + 1 < cw) cp[1] = acc[j][2 * hh + 1];
+                        }
+                    }
                 }
             }
             __syncthreads();
@@ -256,7 +310,7 @@ __device__ void batch_solve_blocked(double *A, long ld, int n, int nrhs, int pw,
     if (tid == 0) *info = first_zero;
 }
 
-__global__ void batch_lu_kernel(double *data, const BatchSys *sys, const int *order, int count, int *counter,
+__global__ void __launch_bounds__(512, 2) batch_lu_kernel(double *data, const BatchSys *sys, const int *order, int count, int *counter,
                                 int *info, int pw, long smem_doubles)
 {
     extern __shared__ double bsm[];
@@ -278,7 +332,8 @@ __global__ void batch_lu_kernel(double *data, const BatchSys *sys, const int *or
             batch_solve_smem(A, S.ld, S.n, S.nrhs, bsm, info + i, s_v, s_i);
         } else {
             // panel (n x pw) then the U chunk (pw x 64)
-            batch_solve_blocked(A, S.ld, S.n, S.nrhs, pw, bsm, bsm + (size_t)S.n * pw, s_piv, s_dinv, info + i, s_v,
+            batch_solve_blocked(A, S.ld, S.n, S.nrhs, pw, bsm, bsm + (size_t)S.n * (pw + BATCH_PANEL_PAD), s_piv, s_dinv,
+                                info + i, s_v,
                                 s_i);
         }
         __syncthreads();
@@ -287,13 +342,15 @@ __global__ void batch_lu_kernel(double *data, const BatchSys *sys, const int *or
 
 long batch_smem_doubles(const BatchSys *sys, int count, int pw)
 {
-    // blocked path of system i: its panel (n x pw) then either the U chunk
-    // (pw x 64) or, in the back substitution, y (n x nrhs) then a 32 x 33
-    // diagonal block; the in-shared-memory path uses whatever this leaves
+    // blocked path of system i: its panel (n x (pw + pad)) then either the U
+    // chunk (pw x BATCH_U_STRIDE) or, in the back substitution, y (n x nrhs)
+    // then a 32 x 33 diagonal block; the in-shared-memory path uses whatever
+    // this leaves
     long need = 0;
-    const long tail = pw * 64 > 32 * 33 ? pw * 64 : 32 * 33;
+    const long tail = pw * BATCH_U_STRIDE > 32 * 33 ? pw * BATCH_U_STRIDE : 32 * 33;
+    const long ps = pw + BATCH_PANEL_PAD;
     for (int i = 0; i < count; i++) {
-        const long w = sys[i].nrhs > pw ? sys[i].nrhs : pw;
+        const long w = sys[i].nrhs > ps ? sys[i].nrhs : ps;
         const long ni = (long)sys[i].n * w + tail;
         if (ni > need) need = ni;
     }
@@ -302,7 +359,7 @@ long batch_smem_doubles(const BatchSys *sys, int count, int pw)
 
 cudaError_t batch_lu_grid(int threads, long smem_doubles, int ctas_per_sm, int count, int *grid)
 {
-    if (threads < 64 || threads > 1024 || (threads & 31)) return cudaErrorInvalidValue;
+    if (threads < 64 || threads > 512 || (threads & 31)) return cudaErrorInvalidValue;
     const size_t smem = (size_t)smem_doubles * sizeof(double);
     if (smem > BATCH_SMEM_MAX) return cudaErrorInvalidValue;
     cudaError_t e = cudaFuncSetAttribute(batch_lu_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, BATCH_SMEM_MAX);
@@ -324,7 +381,7 @@ cudaError_t launch_batch_lu(double *data, const BatchSys *sys, const int *order,
                             long smem_doubles, int pw, int threads, int grid, cudaStream_t st)
 {
     if (count <= 0) return cudaSuccess;
-    if (pw < 16 || pw > 64 || threads < 64 || threads > 1024 || (threads & 31) || grid < 1 ||
+    if (pw < 16 || pw > 64 || threads < 64 || threads > 512 || (threads & 31) || grid < 1 ||
         (size_t)smem_doubles * sizeof(double) > BATCH_SMEM_MAX)
         return cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), st);

@@ -1929,8 +1929,8 @@ extern "C" int lu2gpu_batch_iterations(lu2gpu_batch *b, int *iters_host)
 
 extern "C" int lu2gpu_batch_set_config(lu2gpu_batch *b, int threads, int pw, int ctas_per_sm)
 {
-    if (!b || threads < 64 || threads > 1024 || (threads & 31) || pw < 16 || pw > 64 || ctas_per_sm < 1) {
-        set_error("lu2gpu_batch_set_config: threads in [64,1024] (multiple of 32), pw in [16,64], ctas >= 1");
+    if (!b || threads < 64 || threads > 512 || (threads & 31) || pw < 16 || pw > 64 || ctas_per_sm < 1) {
+        set_error("lu2gpu_batch_set_config: threads in [64,512] (multiple of 32), pw in [16,64], ctas >= 1");
         return LU2GPU_ERR_ARG;
     }
     DeviceGuard g(b->ctx->device);
