@@ -484,6 +484,10 @@ def main() -> int:
                     help="profiling run for ncu: one BF16-LU + IR solve of the diagonally dominant system")
     ap.add_argument("--profile-fp8", action="store_true",
                     help="profiling run for ncu: one FP8-LU + GMRES-IR solve of the diagonally dominant system")
+    ap.add_argument("--profile-batched", action="store_true",
+                    help="profiling run for ncu: one FP64 batched solve of the batch-count systems")
+    ap.add_argument("--batch-config", default=None,
+                    help="threads,panel_width,ctas_per_sm for --profile-batched (default: autotune)")
     ap.add_argument("--no-fp8", action="store_true", help="skip the FP8 + GMRES-IR measurement")
     ap.add_argument("--fp8-n", type=int, default=98304)
     ap.add_argument("--fp8-nb", type=int, default=256)
@@ -530,6 +534,28 @@ def main() -> int:
     ctx = L.Context(local)
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
+    if args.profile_batched:
+        n_b, r_b = L.batch_sizes(args.batch_count, 1, 16, 512, 0.1, 8)
+        b = L.Batch(ctx, n_b, r_b)
+        b.generate_seeds(1 + np.arange(args.batch_count))
+        if args.batch_config:
+            t_, pw_, g_ = (int(v) for v in args.batch_config.split(","))
+            b.set_config(t_, pw_, g_)
+            cfg = {"threads": t_, "pw": pw_, "ctas_per_sm": g_}
+        else:
+            b.snapshot()
+            cfg = b.autotune()
+            b.restore()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        info = b.solve()
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_batched_s": time.perf_counter() - t0, "count": args.batch_count,
+                          "config": cfg, "zero_pivots": int((info != 0).sum()),
+                          "max_hpl_residual": float(b.residuals().max())}))
+        b.close()
+        ctx.close()
+        return 0
     ld = L.device_ld(n)
     pristine = torch.empty((n, ld), dtype=torch.float64, device=dev)
     A = torch.empty_like(pristine)

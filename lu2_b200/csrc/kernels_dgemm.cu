@@ -104,7 +104,6 @@ struct GemmParams {
     long ldc;
     double alpha, beta;
     int tiles_m, tiles_n, group_m;
-    int vec_ok;  // C(0,0) 16-byte aligned and ldc even
     int *status;
 };
 
@@ -348,7 +347,6 @@ static cudaError_t gemm_dispatch(const double *a, long lda, long a_rows, long a_
     p.a_y0 = a_row0;
     p.b_x0 = 0;
     p.b_y0 = 0;
-    p.vec_ok = ((reinterpret_cast<uintptr_t>(p.C) & 15) == 0 && (p.ldc & 1) == 0) ? 1 : 0;
     if (narrow) return run_gemm<LU2_GEMM_NARROW, MODE>(ta, tb, p, st);
     if (wide == 1) return run_gemm<LU2_GEMM_WIDE2, MODE>(ta, tb, p, st);
     return run_gemm<LU2_GEMM_WIDE, MODE>(ta, tb, p, st);

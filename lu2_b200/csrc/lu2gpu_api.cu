@@ -635,7 +635,6 @@ extern "C" int lu2gpu_dgemm_dev(lu2gpu_ctx *c, int m, int n, int k, double alpha
 static std::mutex g_mu;
 static lu2gpu_ctx *g_ctx = nullptr;
 static int g_board = 0;
-static int g_nboards = 1;
 static int g_pivot_mode = LU2GPU_PIVOT_PARTIAL;
 static int g_gdr_ok = 0;
 
@@ -769,7 +768,8 @@ extern "C" void gdrsetboardid(int boardid)
     g_board = boardid;
 }
 
-extern "C" void gdrsetnboards(int nboards) { g_nboards = nboards > 0 ? nboards : 1; }
+// one GPU per process: the board count of the multi-board GRAPE-DR host has no meaning here
+extern "C" void gdrsetnboards(int nboards) { (void)nboards; }
 extern "C" void gdrsetforceswapab(void) {}
 extern "C" void gdrresetforceswapab(void) {}
 extern "C" void gdrsetskipsendjmat(void) {}
