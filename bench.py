@@ -538,12 +538,12 @@ def main() -> int:
         n_b, r_b = L.batch_sizes(args.batch_count, 1, 16, 512, 0.1, 8)
         b = L.Batch(ctx, n_b, r_b)
         b.generate_seeds(1 + np.arange(args.batch_count))
+        b.snapshot()  # the original systems, for the residuals
         if args.batch_config:
             t_, pw_, g_ = (int(v) for v in args.batch_config.split(","))
             b.set_config(t_, pw_, g_)
             cfg = {"threads": t_, "pw": pw_, "ctas_per_sm": g_}
         else:
-            b.snapshot()
             cfg = b.autotune()
             b.restore()
         torch.cuda.synchronize()

@@ -71,6 +71,15 @@ struct lu2gpu_ctx {
     int *d_status = nullptr;
     double *d_bt = nullptr;
     size_t bt_cap = 0;  // doubles
+    // transposed U blocks of the updates inside a panel, apart from d_bt so
+    // that a panel can be factored while the previous step's update reads d_bt
+    double *d_btp = nullptr;
+    size_t btp_cap = 0;
+    // lookahead of the FP64 factorization: the next panel on a high-priority stream
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_cols = nullptr, ev_panel = nullptr;
+    // every buffer comes from fixed scratch (lu2gpu_lusolve_noalloc): nothing is allocated
+    bool fixed_scratch = false;
     int *d_ipiv = nullptr;
     double *d_dinv = nullptr;
     size_t piv_cap = 0;
@@ -84,6 +93,10 @@ struct lu2gpu_ctx {
     // copies of finished factor blocks to pinned host memory during the factorization
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t copy_ev = nullptr;
+    // host-to-device copies of column chunks of a pinned host matrix, one
+    // event per chunk, overlapped with the left-looking start of the factorization
+    cudaStream_t h2d_stream = nullptr;
+    std::vector<cudaEvent_t> h2d_ev;
     // phase timers
     bool timing = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[PH_COUNT];
@@ -197,6 +210,13 @@ extern "C" int lu2gpu_destroy(lu2gpu_ctx *c)
     cudaFree(c->d_status);
     cudaFree(c->leaf.slots);
     cudaFree(c->d_bt);
+    cudaFree(c->d_btp);
+    if (c->side) {
+        cudaStreamSynchronize(c->side);
+        cudaStreamDestroy(c->side);
+    }
+    if (c->ev_cols) cudaEventDestroy(c->ev_cols);
+    if (c->ev_panel) cudaEventDestroy(c->ev_panel);
     cudaFree(c->d_ipiv);
     cudaFree(c->d_dinv);
     for (int i = 0; i < 4; i++) cudaFree(c->d_stage[i]);
@@ -205,6 +225,11 @@ extern "C" int lu2gpu_destroy(lu2gpu_ctx *c)
         cudaStreamDestroy(c->copy_stream);
     }
     if (c->copy_ev) cudaEventDestroy(c->copy_ev);
+    if (c->h2d_stream) {
+        cudaStreamSynchronize(c->h2d_stream);
+        cudaStreamDestroy(c->h2d_stream);
+    }
+    for (cudaEvent_t e : c->h2d_ev) cudaEventDestroy(e);
     free_mixed(c);
     for (int p = 0; p < PH_COUNT; p++)
         for (auto &e : c->ev[p]) {
@@ -362,15 +387,39 @@ static int right_part(lu2gpu_ctx *c, const View &v, int k0, int k1, int cs, int 
         PhaseTimer t(c, top ? PH_SWAP : PH_PANEL);
         K_TRY(launch_laswp_scale(v.a, v.ld, k0, k1, ipiv, v.goff, dinv, cs, ce, true, c->stream));
     }
+    double *bt = (!top && c->d_btp) ? c->d_btp : c->d_bt;
     {
         PhaseTimer t(c, top ? PH_TRSM : PH_PANEL);
-        K_TRY(launch_trsm_unit_lower(v.a, v.ld, k0, K, cs, ce, c->d_bt, c->stream));
+        K_TRY(launch_trsm_unit_lower(v.a, v.ld, k0, K, cs, ce, bt, c->stream));
     }
     if (k1 < v.n) {
         PhaseTimer t(c, top ? PH_DGEMM : PH_PANEL);
-        K_TRY(launch_dgemm_update(v.a, v.ld, v.n, k1, k0, c->d_bt, v.a + (size_t)k1 * v.ld + cs, v.ld, v.n - k1,
+        K_TRY(launch_dgemm_update(v.a, v.ld, v.n, k1, k0, bt, v.a + (size_t)k1 * v.ld + cs, v.ld, v.n - k1,
                                   ce - cs, K, c->d_status, c->stream));
     }
+    return 0;
+}
+
+// right_part (top level, no phase timers) with the update's columns split at
+// cs + w1: `hook` runs between the update of columns cs..cs+w1-1 and that of
+// the rest (the lookahead factors the next panel there)
+template <typename Hook>
+static int right_part_split(lu2gpu_ctx *c, const View &v, int k0, int k1, int cs, int ce, int w1, Hook hook)
+{
+    if (ce <= cs) return hook();
+    const int K = k1 - k0;
+    K_TRY(launch_laswp_scale(v.a, v.ld, k0, k1, c->d_ipiv + v.goff, v.goff, c->d_dinv + v.goff, cs, ce, true,
+                             c->stream));
+    K_TRY(launch_trsm_unit_lower(v.a, v.ld, k0, K, cs, ce, c->d_bt, c->stream));
+    if (k1 >= v.n) return hook();
+    if (w1 > ce - cs) w1 = ce - cs;
+    double *C = v.a + (size_t)k1 * v.ld + cs;
+    K_TRY(launch_dgemm_update(v.a, v.ld, v.n, k1, k0, c->d_bt, C, v.ld, v.n - k1, w1, K, c->d_status, c->stream));
+    const int rc = hook();
+    if (rc) return rc;
+    if (w1 < ce - cs)
+        K_TRY(launch_dgemm_update(v.a, v.ld, v.n, k1, k0, c->d_bt + (size_t)w1 * K, C + w1, v.ld, v.n - k1,
+                                  ce - cs - w1, K, c->d_status, c->stream));
     return 0;
 }
 
@@ -403,7 +452,9 @@ static int ensure_work(lu2gpu_ctx *c, int n, int ncols, int nb)
     size_t need_bt = (size_t)ncols * (size_t)nb + 1024;
     int rc = grow((void **)&c->d_bt, &c->bt_cap, need_bt * sizeof(double));
     if (rc) return rc;
-    c->bt_cap = c->bt_cap;  // bytes
+    if (!c->fixed_scratch &&
+        (rc = grow((void **)&c->d_btp, &c->btp_cap, ((size_t)nb * nb + 1024) * sizeof(double))))
+        return rc;
     if (c->piv_cap < (size_t)n) {
         cudaFree(c->d_ipiv);
         cudaFree(c->d_dinv);
@@ -456,19 +507,113 @@ static int gpu_panel_width(int m)
     return w;
 }
 
+// Lookahead of the FP64 factorization (the reference's lu_mpi_blocked_lookahead
+// idea, lu2_mpi.c:3643-3847, on one GPU): step k updates the next panel's
+// columns first, then that panel is factored on a high-priority stream while
+// the rest of step k's update runs; step k+1's right part waits for it (its
+// row exchanges cross the columns the update wrote).  The panel's own updates
+// use their own transposed-U buffer (d_btp).  Every element sees the same
+// operations in the same order as in the serial schedule: bit-identical.
+// Serial when phase timing is on (the phase split stays meaningful), for
+// fewer than four panels, on fixed scratch, or with LU2GPU_LOOKAHEAD=0.
+static bool use_lookahead(const lu2gpu_ctx *c, int rows, int nb)
+{
+    const char *env = getenv("LU2GPU_LOOKAHEAD");
+    return !c->timing && !c->fixed_scratch && c->d_btp && rows >= 4 * nb && !(env && env[0] == '0');
+}
+
+template <typename AfterStep>
+static int factor_lookahead(lu2gpu_ctx *c, const View &v, int i0, int nb, int mode, AfterStep after_step)
+{
+    const int n = v.n;
+    if (!c->side) {
+        int least = 0, greatest = 0;
+        CU_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        CU_TRY(cudaStreamCreateWithPriority(&c->side, cudaStreamNonBlocking, greatest));
+        CU_TRY(cudaEventCreateWithFlags(&c->ev_cols, cudaEventDisableTiming));
+        CU_TRY(cudaEventCreateWithFlags(&c->ev_panel, cudaEventDisableTiming));
+    }
+    const cudaStream_t main_st = c->stream;
+    int rc = panel(c, v, i0, std::min(nb, n - i0), mode);  // the first panel, on the main stream
+    for (int i = i0; rc == 0 && i < n; i += nb) {
+        const int w = std::min(nb, n - i), i1 = i + w, w1 = std::min(nb, n - i1);
+        if (i > i0 && cudaStreamWaitEvent(main_st, c->ev_panel, 0) != cudaSuccess) {
+            set_error("lookahead: cudaStreamWaitEvent failed");
+            rc = LU2GPU_ERR_CUDA;
+            break;
+        }
+        auto next_panel = [&]() -> int {
+            if (i1 >= n) return 0;
+            CU_TRY(cudaEventRecord(c->ev_cols, main_st));
+            CU_TRY(cudaStreamWaitEvent(c->side, c->ev_cols, 0));
+            c->stream = c->side;
+            const int r = panel(c, v, i1, w1, mode);
+            c->stream = main_st;
+            if (r) return r;
+            CU_TRY(cudaEventRecord(c->ev_panel, c->side));
+            return 0;
+        };
+        rc = right_part_split(c, v, i, i1, i1, v.ncols, w1, next_panel);
+        if (!rc) rc = after_step(i, w);
+    }
+    c->stream = main_st;
+    // everything on the panel stream precedes what follows on the main stream
+    if (cudaEventRecord(c->ev_panel, c->side) != cudaSuccess ||
+        cudaStreamWaitEvent(main_st, c->ev_panel, 0) != cudaSuccess) {
+        cudaGetLastError();
+        if (!rc) {
+            set_error("lookahead: joining the panel stream failed");
+            rc = LU2GPU_ERR_CUDA;
+        }
+    }
+    return rc;
+}
+
 // `after_step(i, w)`, if given, runs once the enqueue of panel step i..i+w-1
 // is complete (rows i..i+w-1 from column i, and columns i..i+w-1 below them,
 // hold their final values once that work has executed: later steps touch
-// neither, lu2.c:543-553)
-template <typename AfterStep>
-static int factor_enqueue_with(lu2gpu_ctx *c, int n, int nrhs, double *a, long lda, int nb, int mode,
-                               AfterStep after_step)
+// neither, lu2.c:543-553).
+//
+// `wait_cols(ce)` makes the compute stream wait until columns 0..ce-1 of the
+// matrix are on the device.  While they arrive, the first `p0` panels are
+// factored left-looking: panel p's columns receive the updates of panels
+// 0..p-1 (the same row exchanges, U-block solve and GEMM per element, in the
+// same panel order, as the right-looking steps apply to them) and are
+// factored; the columns right of panel p0 then catch up in arrival order,
+// `group` columns at a time, and the right-looking loop continues from panel
+// p0.  Factors and pivots are bit-identical to the right-looking schedule.
+template <typename AfterStep, typename WaitCols>
+static int factor_enqueue_arriving(lu2gpu_ctx *c, int n, int nrhs, double *a, long lda, int nb, int mode, int p0,
+                                   int group, AfterStep after_step, WaitCols wait_cols)
 {
     if (nb > NB_MAX) nb = NB_MAX;
     int rc = ensure_work(c, n, n + nrhs, nb);
     if (rc) return rc;
     View v{a, lda, n, n + nrhs, 0};
-    for (int i = 0; i < n; i += nb) {
+    const int ncol = n + nrhs;
+    int i0 = 0;  // columns 0..i0-1 factored left-looking
+    for (int p = 0; p < p0 && i0 < n; ++p) {
+        const int w = (n - i0) < nb ? (n - i0) : nb;
+        if ((rc = wait_cols(i0 + w))) return rc;
+        for (int k = 0; k < i0; k += nb)
+            if ((rc = right_part(c, v, k, k + nb, i0, i0 + w, true))) return rc;
+        if ((rc = panel(c, v, i0, w, mode))) return rc;
+        i0 += w;
+    }
+    if (i0 > 0) {
+        if (group < nb) group = nb;
+        for (int cs = i0; cs < ncol; cs += group) {
+            const int ce = (ncol - cs) < group ? ncol : cs + group;
+            if ((rc = wait_cols(ce))) return rc;
+            for (int k = 0; k < i0; k += nb)
+                if ((rc = right_part(c, v, k, (i0 - k) < nb ? i0 : k + nb, cs, ce, true))) return rc;
+        }
+        for (int k = 0; k < i0; k += nb)
+            if ((rc = after_step(k, (i0 - k) < nb ? i0 - k : nb))) return rc;
+    }
+    if ((rc = wait_cols(ncol))) return rc;
+    if (i0 < n && use_lookahead(c, n - i0, nb)) return factor_lookahead(c, v, i0, nb, mode, after_step);
+    for (int i = i0; i < n; i += nb) {
         const int w = (n - i) < nb ? (n - i) : nb;
         rc = panel(c, v, i, w, mode);
         if (rc) return rc;
@@ -477,6 +622,13 @@ static int factor_enqueue_with(lu2gpu_ctx *c, int n, int nrhs, double *a, long l
         if ((rc = after_step(i, w))) return rc;
     }
     return 0;
+}
+
+template <typename AfterStep>
+static int factor_enqueue_with(lu2gpu_ctx *c, int n, int nrhs, double *a, long lda, int nb, int mode,
+                               AfterStep after_step)
+{
+    return factor_enqueue_arriving(c, n, nrhs, a, lda, nb, mode, 0, 0, after_step, [](int) { return 0; });
 }
 
 static int factor_enqueue(lu2gpu_ctx *c, int n, int nrhs, double *a, long lda, int nb, int mode)
@@ -881,6 +1033,26 @@ extern "C" void reset_gdr(int m, double *a, int nb, double *awork, int n)
 
 // ----- lu2.c: lumcolumn -----
 
+// Panels to factor left-looking while a pinned host matrix streams in: the
+// fewest whose work outlasts the copy of its 8 n^2 bytes at ~50 GB/s, counting
+// 2 (n - (k+1) nb) nb^2 FLOPs at ~30 TFLOP/s for each earlier panel k's update
+// of a panel's columns and ~6 us per column for the panel itself.  Fewer only
+// leaves the later column groups waiting for their copies; more only runs
+// more of the start as narrow (one-panel-wide) updates.
+static int left_looking_panels(int n, int nb)
+{
+    const double t_copy = 8.0 * n * (double)(n + 1) / 50e9;
+    const int panels = (n + nb - 1) / nb;
+    double t = 0;
+    int p = 0;
+    while (p < panels && t < t_copy) {
+        for (int k = 0; k < p; ++k) t += 2.0 * (n - (k + 1.0) * nb) * (double)nb * nb / 30e12;
+        t += nb * 6e-6;
+        ++p;
+    }
+    return p;
+}
+
 // lumcolumn (lu2.c:1122-1144) on the caller's host matrix a[n][n+16] (b in
 // column n): the matrix goes to the GPU, is factored there (recursive panels,
 // nb = m), x = U'^{-1} y is written to b, the factored matrix (with y in
@@ -921,9 +1093,46 @@ static int lumcolumn_host(int n, double *a, double *b, int m, int *pv)
         CU_TRY(cudaEventCreateWithFlags(&c->copy_ev, cudaEventDisableTiming));
     }
     if ((rc = begin_status(c))) return rc;
-    CU_TRY(cudaMemcpy2DAsync(d, ld * sizeof(double), a, rdim * sizeof(double), (size_t)(n + 1) * sizeof(double), n,
-                             cudaMemcpyHostToDevice, c->stream));
     const size_t pitch_h = rdim * sizeof(double), pitch_d = ld * sizeof(double);
+    // pinned host matrix: column chunks go to the device on their own stream,
+    // one event each, and the factorization starts left-looking on the chunks
+    // that have arrived (factor_enqueue_arriving); pageable: one copy first
+    const int ncol = n + 1;
+    const char *ov = getenv("LU2GPU_H2D_OVERLAP");
+    const bool overlap = pinned && !(ov && atoi(ov) == 0);
+    int cw = ncol, p0 = 0, group = 0, waited = 0;
+    if (overlap) {
+        if (!c->h2d_stream) CU_TRY(cudaStreamCreateWithFlags(&c->h2d_stream, cudaStreamNonBlocking));
+        cw = (512 / nbw) * nbw;  // >= 4 KB per row segment; nbw <= 512
+        const int nchunk = (ncol + cw - 1) / cw;
+        while ((int)c->h2d_ev.size() < nchunk) {
+            cudaEvent_t e;
+            CU_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            c->h2d_ev.push_back(e);
+        }
+        // the staging matrix is rewritten only after the stream's earlier work on it
+        CU_TRY(cudaEventRecord(c->copy_ev, c->stream));
+        CU_TRY(cudaStreamWaitEvent(c->h2d_stream, c->copy_ev, 0));
+        for (int j = 0; j < nchunk; ++j) {
+            const int c0 = j * cw, w = (ncol - c0) < cw ? ncol - c0 : cw;
+            CU_TRY(cudaMemcpy2DAsync(d + c0, pitch_d, a + c0, pitch_h, (size_t)w * sizeof(double), n,
+                                     cudaMemcpyHostToDevice, c->h2d_stream));
+            CU_TRY(cudaEventRecord(c->h2d_ev[j], c->h2d_stream));
+        }
+        const char *lp = getenv("LU2GPU_LEFT_PANELS");
+        p0 = lp ? atoi(lp) : left_looking_panels(n, nbw);
+        group = (4096 / cw) * cw;
+        if (group < cw) group = cw;
+    } else {
+        CU_TRY(cudaMemcpy2DAsync(d, pitch_d, a, pitch_h, (size_t)ncol * sizeof(double), n, cudaMemcpyHostToDevice,
+                                 c->stream));
+    }
+    auto wait_cols = [&](int ce) -> int {
+        if (!overlap) return 0;
+        for (const int need = (ce + cw - 1) / cw; waited < need; ++waited)
+            CU_TRY(cudaStreamWaitEvent(c->stream, c->h2d_ev[waited], 0));
+        return 0;
+    };
     auto copy_back = [&](int i, int w) -> int {
         if (!pinned) return 0;
         CU_TRY(cudaEventRecord(c->copy_ev, c->stream));
@@ -936,7 +1145,8 @@ static int lumcolumn_host(int n, double *a, double *b, int m, int *pv)
                                      (size_t)w * sizeof(double), n - i - w, cudaMemcpyDeviceToHost, c->copy_stream));
         return 0;
     };
-    if ((rc = factor_enqueue_with(c, n, 1, d, ld, nbw, g_pivot_mode, copy_back))) return rc;
+    if ((rc = factor_enqueue_arriving(c, n, 1, d, ld, nbw, g_pivot_mode, p0, group, copy_back, wait_cols)))
+        return rc;
     CU_TRY(cudaMemcpy2DAsync(x, sizeof(double), d + n, ld * sizeof(double), sizeof(double), n,
                              cudaMemcpyDeviceToDevice, c->stream));
     {
@@ -1351,6 +1561,7 @@ extern "C" int lu2gpu_lusolve_noalloc(int n, int nrhs, double *a, long lda, int 
     c.piv_cap = NOALLOC_MAX_N;
     c.d_bt = (double *)(base + NA_BT);
     c.bt_cap = NA_BT_BYTES;
+    c.fixed_scratch = true;
 
     // The status words must start cleared (begin_status); the leaf barrier
     // counter is cleared before every leaf launch.  Pivots, 1/pivot and the U

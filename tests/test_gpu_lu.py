@@ -110,6 +110,50 @@ def test_lumcolumn_pinned_host_overlaps_copies(oracle, n, nb):
     np.testing.assert_array_equal(pv_pin, pv_pg)
 
 
+@pytest.mark.parametrize("n,nb,mode", [(2000, 128, PIVOT_PARTIAL), (1111, 64, PIVOT_PARTIAL), (3000, 256, PIVOT_REF),
+                                       (2048, 512, PIVOT_PARTIAL)])
+def test_lookahead_matches_serial_factorization(ctx, monkeypatch, n, nb, mode):
+    """The lookahead schedule (the next panel factored on a high-priority
+    stream while the rest of the update runs) gives the serial schedule's
+    factors, right-hand side and pivots bit for bit."""
+    out = []
+    for env in ("0", "1"):
+        monkeypatch.setenv("LU2GPU_LOOKAHEAD", env)
+        a, ld = dev_matrix(ctx, n, 21)
+        assert ctx.lusolve(a, n, ld, nb, 1, mode) == 0
+        out.append((a.cpu().numpy()[:, : n + 1], ctx.pivots(n)))
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    np.testing.assert_array_equal(out[0][1], out[1][1])
+
+
+@pytest.mark.parametrize("n,nb,left", [(1500, 128, 3), (1500, 128, 100), (1000, 48, 7), (300, 256, 2),
+                                       (37, 16, 1)])
+def test_lumcolumn_left_looking_start_is_bit_identical(oracle, monkeypatch, n, nb, left):
+    """On pinned host buffers the matrix arrives in column chunks and the
+    first panels are factored left-looking as they arrive (the columns right
+    of them catch up afterwards); every element sees the same operations in
+    the same order as in the right-looking schedule, so the result is the
+    same bit for bit as the pageable path's.  `left` forces the number of
+    left-looking panels (100: all of them)."""
+    import torch
+
+    a_pg = oracle.randomsetmat(n, 9)
+    b_pg = np.zeros(n)
+    pv_pg = np.zeros(nb, dtype=np.int32)
+    assert lumcolumn(a_pg, b_pg, nb, pv_pg, PIVOT_PARTIAL) == 0
+    monkeypatch.setenv("LU2GPU_LEFT_PANELS", str(left))
+    a_t = torch.empty(a_pg.shape, dtype=torch.float64, pin_memory=True)
+    b_t = torch.zeros(n, dtype=torch.float64, pin_memory=True)
+    a_pin, b_pin = a_t.numpy(), b_t.numpy()
+    a_pin[...] = np.nan
+    a_pin[:, : n + 1] = oracle.randomsetmat(n, 9)[:, : n + 1]
+    pv_pin = np.zeros(nb, dtype=np.int32)
+    assert lumcolumn(a_pin, b_pin, nb, pv_pin, PIVOT_PARTIAL) == 0
+    np.testing.assert_array_equal(a_pin[:, : n + 1], a_pg[:, : n + 1])
+    np.testing.assert_array_equal(b_pin, b_pg)
+    np.testing.assert_array_equal(pv_pin, pv_pg)
+
+
 @pytest.mark.parametrize("n,nb", [(1, 16), (2, 16), (15, 16), (16, 16), (17, 16), (33, 16), (100, 32), (1000, 256),
                                   (777, 64)])
 def test_ragged_sizes_vs_lapack(ctx, oracle, n, nb):
