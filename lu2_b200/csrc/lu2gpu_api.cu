@@ -1033,24 +1033,20 @@ extern "C" void reset_gdr(int m, double *a, int nb, double *awork, int n)
 
 // ----- lu2.c: lumcolumn -----
 
-// Panels to factor left-looking while a pinned host matrix streams in: the
-// fewest whose work outlasts the copy of its 8 n^2 bytes at ~50 GB/s, counting
-// 2 (n - (k+1) nb) nb^2 FLOPs at ~30 TFLOP/s for each earlier panel k's update
-// of a panel's columns and ~6 us per column for the panel itself.  Fewer only
-// leaves the later column groups waiting for their copies; more only runs
-// more of the start as narrow (one-panel-wide) updates.
+// Panels to factor left-looking while a pinned host matrix streams in: enough
+// that the catch-up of each arriving column group (p0 panel updates, 2 n nb
+// FLOPs per column each at ~30 TFLOP/s) takes as long as the group's copy
+// (8 n bytes per column at ~55 GB/s over PCIe), i.e. p0 = 8 * 30e12 /
+// (55e9 * 2 nb), independent of n.  Fewer leaves the compute waiting for the
+// copy; more runs a growing start as narrow one-panel-wide updates, whose row
+// exchanges and U-block solves cost as much as full-width ones.  Measured at
+// n = 65536, nb = 256 (e2e seconds): p0 = 1: 6.76, 4: 6.57, 9: 6.26,
+// 16: 6.28, 32: 6.39, 64: 6.75; without the chunked copy 6.82.
 static int left_looking_panels(int n, int nb)
 {
-    const double t_copy = 8.0 * n * (double)(n + 1) / 50e9;
     const int panels = (n + nb - 1) / nb;
-    double t = 0;
-    int p = 0;
-    while (p < panels && t < t_copy) {
-        for (int k = 0; k < p; ++k) t += 2.0 * (n - (k + 1.0) * nb) * (double)nb * nb / 30e12;
-        t += nb * 6e-6;
-        ++p;
-    }
-    return p;
+    const int p0 = (int)ceil(8.0 * 30e12 / (55e9 * 2.0 * nb));
+    return p0 < panels ? p0 : panels;
 }
 
 // lumcolumn (lu2.c:1122-1144) on the caller's host matrix a[n][n+16] (b in
