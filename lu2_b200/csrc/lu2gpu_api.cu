@@ -516,6 +516,14 @@ static int gpu_panel_width(int m)
 // operations in the same order as in the serial schedule: bit-identical.
 // Serial when phase timing is on (the phase split stays meaningful), for
 // fewer than four panels, on fixed scratch, or with LU2GPU_LOOKAHEAD=0.
+//
+// A panel factored beside the update holds its leaf to LOOKAHEAD_LEAF_CTAS
+// CTAs (more if its slab needs them): each leaf CTA takes the place of one of
+// the update's two CTAs on an SM, and the leaf is bound by its per-column
+// exchange, not its CTA count.  Measured at N=65536 (TFLOP/s, leaf capped
+// everywhere): 148 CTAs 30.36, 96 30.78, 64 31.03, 48 31.02.
+constexpr int LOOKAHEAD_LEAF_CTAS = 64;
+
 static bool use_lookahead(const lu2gpu_ctx *c, int rows, int nb)
 {
     const char *env = getenv("LU2GPU_LOOKAHEAD");
@@ -534,6 +542,7 @@ static int factor_lookahead(lu2gpu_ctx *c, const View &v, int i0, int nb, int mo
         CU_TRY(cudaEventCreateWithFlags(&c->ev_panel, cudaEventDisableTiming));
     }
     const cudaStream_t main_st = c->stream;
+    const int all_ctas = c->leaf_ctas;
     int rc = panel(c, v, i0, std::min(nb, n - i0), mode);  // the first panel, on the main stream
     for (int i = i0; rc == 0 && i < n; i += nb) {
         const int w = std::min(nb, n - i), i1 = i + w, w1 = std::min(nb, n - i1);
@@ -547,8 +556,10 @@ static int factor_lookahead(lu2gpu_ctx *c, const View &v, int i0, int nb, int mo
             CU_TRY(cudaEventRecord(c->ev_cols, main_st));
             CU_TRY(cudaStreamWaitEvent(c->side, c->ev_cols, 0));
             c->stream = c->side;
+            c->leaf_ctas = std::min(all_ctas, std::max(LOOKAHEAD_LEAF_CTAS, leaf_min_ctas(n - i1, sizeof(double))));
             const int r = panel(c, v, i1, w1, mode);
             c->stream = main_st;
+            c->leaf_ctas = all_ctas;
             if (r) return r;
             CU_TRY(cudaEventRecord(c->ev_panel, c->side));
             return 0;
@@ -557,6 +568,7 @@ static int factor_lookahead(lu2gpu_ctx *c, const View &v, int i0, int nb, int mo
         if (!rc) rc = after_step(i, w);
     }
     c->stream = main_st;
+    c->leaf_ctas = all_ctas;
     // everything on the panel stream precedes what follows on the main stream
     if (cudaEventRecord(c->ev_panel, c->side) != cudaSuccess ||
         cudaStreamWaitEvent(main_st, c->ev_panel, 0) != cudaSuccess) {

@@ -111,11 +111,12 @@ def test_lumcolumn_pinned_host_overlaps_copies(oracle, n, nb):
 
 
 @pytest.mark.parametrize("n,nb,mode", [(2000, 128, PIVOT_PARTIAL), (1111, 64, PIVOT_PARTIAL), (3000, 256, PIVOT_REF),
-                                       (2048, 512, PIVOT_PARTIAL)])
+                                       (2048, 512, PIVOT_PARTIAL), (12000, 256, PIVOT_PARTIAL)])
 def test_lookahead_matches_serial_factorization(ctx, monkeypatch, n, nb, mode):
     """The lookahead schedule (the next panel factored on a high-priority
-    stream while the rest of the update runs) gives the serial schedule's
-    factors, right-hand side and pivots bit for bit."""
+    stream while the rest of the update runs, its leaf on fewer CTAs once the
+    rows need more than 64) gives the serial schedule's factors, right-hand
+    side and pivots bit for bit."""
     out = []
     for env in ("0", "1"):
         monkeypatch.setenv("LU2GPU_LOOKAHEAD", env)
