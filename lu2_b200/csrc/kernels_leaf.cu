@@ -11,13 +11,15 @@
 //
 // Per column the critical path is one exchange between CTAs: every CTA
 // publishes its candidate (largest |a| among its rows, its row values, and --
-// from the CTA owning row c -- row c itself) in a slot stamped with a 64-bit
-// sequence number (release store).  Warp 0 of every CTA waits for all slots
-// (each lane re-polls the slots it still waits for with back-to-back relaxed
-// loads, then one acquire fence), reduces them to the same winner, and after
-// a CTA barrier every warp fetches the winner's row and updates its own rows.
-// (Copying every candidate row into every CTA instead, which saves one L2 round
-// trip, measured slower: 148 CTAs reading the same 148 slot lines each column.)
+// from the CTA owning row c -- row c itself) in a slot whose every 64-bit word
+// carries the column's 32-bit stamp beside 32 bits of payload (relaxed
+// stores, no fence).  Warp 0 of every CTA polls the slots' heads (each lane
+// re-loads the heads it still waits for back to back; a head whose words all
+// carry the stamp is complete and already holds the candidate), reduces them
+// to the same winner, loads the winner's row and row c (stamp-checked, re-read
+// until complete) into shared memory, and after a CTA barrier every warp
+// updates its own rows.  (Copying every candidate row into every CTA instead
+// measured slower: 148 CTAs reading the same 148 slot lines each column.)
 // Each thread owns fixed slab rows, so the exchange, the swap, the rank-1
 // update and the next column's local argmax need two CTA barriers per column.
 // Slots are double-buffered by column parity: a CTA can be at most one column
@@ -48,16 +50,30 @@ struct LeafParams {
     int *status;
 };
 
-__device__ __forceinline__ void st_release_u64(unsigned long long *p, unsigned long long v)
+// The 32-bit stamp of publication `seq` (never 0, the value of unwritten slots)
+__device__ __forceinline__ unsigned stamp_of(unsigned long long seq)
 {
-    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+    return (unsigned)(seq % 4294967295ull) + 1u;
 }
 
-__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long *p)
+// a double as two stamped words (high half, low half)
+__device__ __forceinline__ void st_stamped(unsigned long long *p, unsigned tag, double x)
 {
-    unsigned long long v;
-    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-    return v;
+    const unsigned long long b = (unsigned long long)__double_as_longlong(x), t = (unsigned long long)tag << 32;
+    const unsigned long long hi = t | (b >> 32), lo = t | (b & 0xffffffffull);
+    asm volatile("st.relaxed.gpu.global.v2.u64 [%0], {%1, %2};" ::"l"(p), "l"(hi), "l"(lo) : "memory");
+}
+
+__device__ __forceinline__ void ld_pair(const unsigned long long *p, unsigned long long &a, unsigned long long &b)
+{
+    asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];" : "=l"(a), "=l"(b) : "l"(p) : "memory");
+}
+
+__device__ __forceinline__ bool stamped(unsigned long long w, unsigned tag) { return (unsigned)(w >> 32) == tag; }
+
+__device__ __forceinline__ double unstamp(unsigned long long hi, unsigned long long lo)
+{
+    return __longlong_as_double((long long)((hi << 32) | (lo & 0xffffffffull)));
 }
 
 // T = double (plain form) or float (the precision form's FP32 panel); the
@@ -74,6 +90,7 @@ __global__ void __launch_bounds__(LEAF_THREADS) leaf_kernel(LeafParams<T> P)
     __shared__ double s_wv[LEAF_WARPS];
     __shared__ int s_wi[LEAF_WARPS];
     __shared__ int s_fail, s_win;
+    __shared__ double s_prow[2 * LEAF_W];  // the column's pivot row, then row c
     const int rb = c0 + bid * rpc;
     const int re = min(P.n, rb + rpc);
     const int nr = max(0, re - rb);
@@ -112,8 +129,9 @@ __global__ void __launch_bounds__(LEAF_THREADS) leaf_kernel(LeafParams<T> P)
 
     for (int ip = 0; ip < w; ip++) {
         const int c = c0 + ip, par = ip & 1;
-        const unsigned long long seq = P.seq0 + (unsigned long long)ip + 1ull;
+        const unsigned tag = stamp_of(P.seq0 + (unsigned long long)ip + 1ull);
         LeafSlot *myslot = P.slots + (size_t)par * G + bid;
+        const int owner_c = (c - c0) / rpc;
 
         // CTA candidate -> warp 0 publishes it (and row c, from its owner)
         warp_argmax(bv, bi);
@@ -127,23 +145,25 @@ __global__ void __launch_bounds__(LEAF_THREADS) leaf_kernel(LeafParams<T> P)
             int i = lane < LEAF_WARPS ? s_wi[lane] : INT_MAX;
             warp_argmax(v, i);
             if (lane < LEAF_W) {
-                myslot->row[lane] = (i != INT_MAX) ? slab[(i - rb) * LEAF_LDS + lane] : 0.0;
+                st_stamped(&myslot->row[2 * lane], tag, (i != INT_MAX) ? (double)slab[(i - rb) * LEAF_LDS + lane] : 0.0);
             } else if (c >= rb && c < re) {
-                myslot->rowc[lane - LEAF_W] = slab[(c - rb) * LEAF_LDS + lane - LEAF_W];
+                st_stamped(&myslot->rowc[2 * (lane - LEAF_W)], tag, (double)slab[(c - rb) * LEAF_LDS + lane - LEAF_W]);
             }
             if (lane == 0) {
-                myslot->val = v;
-                myslot->idx = i;
+                st_stamped(&myslot->head[0], tag, v);
+                const unsigned long long t = (unsigned long long)tag << 32;
+                asm volatile("st.relaxed.gpu.global.v2.u64 [%0], {%1, %2};" ::"l"(&myslot->head[2]),
+                             "l"(t | (unsigned)i), "l"(t)
+                             : "memory");
             }
-            __syncwarp();  // the lanes' slot writes precede lane 0's release store
-            if (lane == 0) st_release_u64(&myslot->seq, seq);
         }
 
-        // warp 0 waits for every CTA's candidate of this column and reduces
-        // them to the winner.  Each lane watches up to LEAF_THREADS/32 slots:
-        // it loads all those it still waits for back to back (relaxed), so the
-        // polls overlap instead of costing one L2 round trip each; then one
-        // acquire fence per lane before the candidates are read.
+        // warp 0 waits for every CTA's candidate of this column, reduces them
+        // to the winner and fetches the winner's row and row c into shared
+        // memory.  Each lane watches up to LEAF_THREADS/32 slots: it loads the
+        // heads of all those it still waits for back to back, so the polls
+        // overlap instead of costing one L2 round trip each; a head whose
+        // three words carry this column's stamp is complete.
         if (warp == 0) {
             constexpr int QMAX = LEAF_THREADS / 32;
             const LeafSlot *sl = P.slots + (size_t)par * G;
@@ -154,38 +174,64 @@ __global__ void __launch_bounds__(LEAF_THREADS) leaf_kernel(LeafParams<T> P)
             const unsigned long long t0 = globaltimer_ns();
             unsigned spins = 0;
             bool failed = false;
+            double gv = -1.0;
+            int gi = INT_MAX;
             while (pending) {
-                unsigned long long sv[QMAX];
+                unsigned long long h0[QMAX], h1[QMAX], h2[QMAX], h3[QMAX];
 #pragma unroll
-                for (int k = 0; k < QMAX; k++) sv[k] = ((pending >> k) & 1u) ? ld_relaxed_u64(&sl[lane + 32 * k].seq) : 0ull;
+                for (int k = 0; k < QMAX; k++) {
+                    h0[k] = h1[k] = h2[k] = h3[k] = 0ull;
+                    if ((pending >> k) & 1u) {
+                        ld_pair(&sl[lane + 32 * k].head[0], h0[k], h1[k]);
+                        ld_pair(&sl[lane + 32 * k].head[2], h2[k], h3[k]);
+                    }
+                }
 #pragma unroll
                 for (int k = 0; k < QMAX; k++)
-                    if (((pending >> k) & 1u) && sv[k] == seq) pending &= ~(1u << k);
+                    if (((pending >> k) & 1u) && stamped(h0[k], tag) && stamped(h1[k], tag) && stamped(h2[k], tag)) {
+                        pending &= ~(1u << k);
+                        const double v = unstamp(h0[k], h1[k]);
+                        const int i = (int)(unsigned)(h2[k] & 0xffffffffull);
+                        if (argmax_better(v, i, gv, gi)) {
+                            gv = v;
+                            gi = i;
+                        }
+                    }
                 if (pending && (++spins & 63u) == 0 &&
                     (*(volatile int *)&P.status[1] != 0 || globaltimer_ns() - t0 > WAIT_LIMIT_NS)) {
                     failed = true;
                     break;
                 }
             }
-            if (__any_sync(0xffffffffu, failed)) {
-                if (lane == 0) {
-                    if (*(volatile int *)&P.status[1] == 0) record_error(P.status, ERR_BARRIER_TIMEOUT, 1);
-                    s_fail = 1;
-                }
-            } else {
-                asm volatile("fence.acq_rel.gpu;" ::: "memory");  // acquire side of the slots' release stores
-                double gv = -1.0;
-                int gi = INT_MAX;
-                for (int q = lane; q < G; q += 32) {
-                    const double v = __ldcg(&sl[q].val);
-                    const int i = __ldcg(&sl[q].idx);
-                    if (argmax_better(v, i, gv, gi)) {
-                        gv = v;
-                        gi = i;
+            if (!__any_sync(0xffffffffu, failed)) {
+                warp_argmax(gv, gi);
+                // lanes 0..15: the pivot row (row c itself when there is no
+                // finite candidate: a NaN column keeps row c); lanes 16..31: row c
+                const int p = (gi == INT_MAX) ? c : gi;
+                const int owner_p = (p - c0) / rpc;
+                const unsigned long long *src =
+                    (lane < LEAF_W) ? ((gi == INT_MAX) ? &sl[owner_c].rowc[2 * lane] : &sl[owner_p].row[2 * lane])
+                                    : &sl[owner_c].rowc[2 * (lane - LEAF_W)];
+                unsigned long long hi = 0ull, lo = 0ull;
+                bool ok = false;
+                for (unsigned tries = 1;; tries++) {  // the loop's exits are warp-uniform
+                    ld_pair(src, hi, lo);
+                    ok = stamped(hi, tag) && stamped(lo, tag);
+                    if (__all_sync(0xffffffffu, ok)) break;
+                    const bool late = (tries & 63u) == 0 && (*(volatile int *)&P.status[1] != 0 ||
+                                                             globaltimer_ns() - t0 > WAIT_LIMIT_NS);
+                    if (__any_sync(0xffffffffu, late)) {
+                        failed = true;
+                        break;
                     }
                 }
-                warp_argmax(gv, gi);
+                const int j = (lane < LEAF_W) ? lane : lane - LEAF_W;
+                s_prow[lane] = (j < w && ok) ? unstamp(hi, lo) : 0.0;
                 if (lane == 0) s_win = gi;
+            }
+            if (__any_sync(0xffffffffu, failed) && lane == 0) {
+                if (*(volatile int *)&P.status[1] == 0) record_error(P.status, ERR_BARRIER_TIMEOUT, 1);
+                s_fail = 1;
             }
         }
         __syncthreads();  // S2
@@ -193,25 +239,16 @@ __global__ void __launch_bounds__(LEAF_THREADS) leaf_kernel(LeafParams<T> P)
         const int gi = s_win;
 
         const int p = (gi == INT_MAX) ? c : gi;  // no finite candidate (a NaN column): keep row c
-        const int owner_p = (p - c0) / rpc, owner_c = (c - c0) / rpc;
-        // lanes 0..15: the pivot row (row c itself when there is no finite
-        // candidate); lanes 16..31: old row c
-        double pr = 0.0;
-        if (lane < LEAF_W && lane < w)
-            pr = (gi == INT_MAX) ? __ldcg(&P.slots[(size_t)par * G + owner_c].rowc[lane])
-                                 : __ldcg(&P.slots[(size_t)par * G + owner_p].row[lane]);
-        else if (lane >= LEAF_W && lane - LEAF_W < w)
-            pr = __ldcg(&P.slots[(size_t)par * G + owner_c].rowc[lane - LEAF_W]);
-        const T d = (T)__shfl_sync(0xffffffffu, pr, ip);
+        const T d = (T)s_prow[ip];
         const bool zero = (d == T(0));
         const T inv = zero ? T(1) : T(1) / d;
         T u[LEAF_W];   // scaled pivot row
         T rc[LEAF_W];  // old row c (goes to row p)
 #pragma unroll
         for (int j = 0; j < LEAF_W; j++) {
-            const T x = (T)__shfl_sync(0xffffffffu, pr, j);
+            const T x = (T)s_prow[j];
             u[j] = (j == ip || zero) ? x : x * inv;
-            rc[j] = (T)__shfl_sync(0xffffffffu, pr, LEAF_W + j);
+            rc[j] = (T)s_prow[LEAF_W + j];
         }
         if (bid == 0 && tid == 0) {
             P.ipiv[c] = p + P.goff;

@@ -71,13 +71,14 @@ __device__ __forceinline__ void warp_argmax(double &v, int &i)
 void count_launch(long k = 1);
 
 // One CTA's published pivot candidate for one leaf column.
+// One CTA's publication for one leaf column.  Every 64-bit word carries the
+// column's 32-bit stamp in its high half and 32 bits of payload in its low
+// half, so a reader validates each word it loads by its stamp (each aligned
+// 64-bit access is single-copy atomic) without release/acquire ordering.
 struct __align__(64) LeafSlot {
-    double row[16];          // the candidate row's leaf columns
-    double rowc[16];         // row c (written by the CTA owning row c only)
-    double val;              // |a| of the candidate in the search column
-    int idx;                 // its row (view numbering), INT_MAX if none
-    int pad_;
-    unsigned long long seq;  // publication stamp (release store)
+    unsigned long long head[4];   // |a| of the candidate (high, low halves), its row (INT_MAX if none), unused
+    unsigned long long row[32];   // the candidate row's 16 leaf columns, two words per double
+    unsigned long long rowc[32];  // row c, written by the CTA owning row c only
 };
 
 struct LeafBuffers {
