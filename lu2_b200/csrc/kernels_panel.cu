@@ -179,11 +179,23 @@ __global__ void __launch_bounds__(256) trsm_unit_lower_kernel(const E *T, long l
                 Ts[(r - lb) * TRSM_TLD + cc] = (cc < bk) ? T[(size_t)r * ldt + lb + cc] : 0.0;
         }
         __syncthreads();
-        for (int l = 0; l + 1 < bk; l++) {
-            const E xl = X[(lb + l) * TRSM_LDS + col];
-            for (int r = l + 1 + rg; r < bk; r += 8) X[(lb + r) * TRSM_LDS + col] -= Ts[r * TRSM_TLD + l] * xl;
-            __syncthreads();
+        // the bk x bk unit triangle: one lane of warp 0 per column, in
+        // registers, without barriers (same operations in the same order as
+        // the row-by-row elimination)
+        if (rg == 0) {
+            E xd[TRSM_BK];
+#pragma unroll
+            for (int l = 0; l < TRSM_BK; l++) xd[l] = (l < bk) ? X[(lb + l) * TRSM_LDS + col] : E(0);
+#pragma unroll
+            for (int l = 0; l < TRSM_BK - 1; l++)
+#pragma unroll
+                for (int r = l + 1; r < TRSM_BK; r++)
+                    if (r < bk) xd[r] -= Ts[r * TRSM_TLD + l] * xd[l];
+#pragma unroll
+            for (int l = 0; l < TRSM_BK; l++)
+                if (l < bk) X[(lb + l) * TRSM_LDS + col] = xd[l];
         }
+        __syncthreads();
         E xb[TRSM_BK];
 #pragma unroll
         for (int l = 0; l < TRSM_BK; l++) xb[l] = (l < bk) ? X[(lb + l) * TRSM_LDS + col] : 0.0;

@@ -24,28 +24,56 @@ __global__ void __launch_bounds__(256) backsolve_diag_kernel(const T *a, long ld
                                                              int c0, int nr)
 {
     extern __shared__ __align__(16) unsigned char bs_smem[];
-    T *U = reinterpret_cast<T *>(bs_smem);  // bs x (bs+1)
+    T *U = reinterpret_cast<T *>(bs_smem);  // bs x (bs+1): an odd row pitch, conflict-free column reads
     __shared__ T X[BS_BLOCK][BS_MAXR];
     const int lds = bs + 1;
-    for (int idx = threadIdx.x; idx < bs * bs; idx += blockDim.x) {
-        const int r = idx / bs, c = idx - r * bs;
-        U[r * lds + c] = a[(size_t)(r0 + r) * ld + r0 + c];
+    // the block, PER loads in flight per thread before they are stored
+    constexpr int PER = 16;
+    for (int base = 0; base < bs * bs; base += PER * 256) {
+        T v[PER];
+#pragma unroll
+        for (int q = 0; q < PER; q++) {
+            const int idx = base + q * 256 + (int)threadIdx.x;
+            const int r = idx / bs, c = idx - r * bs;
+            v[q] = (idx < bs * bs) ? a[(size_t)(r0 + r) * ld + r0 + c] : T(0);
+        }
+#pragma unroll
+        for (int q = 0; q < PER; q++) {
+            const int idx = base + q * 256 + (int)threadIdx.x;
+            const int r = idx / bs, c = idx - r * bs;
+            if (idx < bs * bs) U[r * lds + c] = v[q];
+        }
     }
     for (int idx = threadIdx.x; idx < bs * nr; idx += blockDim.x) {
         const int r = idx / nr, c = idx - r * nr;
         X[r][c] = x[(size_t)(r0 + r) * ldx + c0 + c];
     }
     __syncthreads();
+    // one warp per right-hand side, column-oriented: lane l holds rows l,
+    // l+32, l+64, l+96; once x_j is final (its owner lane's value) every row
+    // i < j subtracts U'[i][j] x_j
+    constexpr int QB = BS_BLOCK / 32;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int c = warp; c < nr; c += blockDim.x >> 5) {
-        for (int j = bs - 1; j >= 0; j--) {
-            T s = 0;
-            for (int k = j + 1 + lane; k < bs; k += 32) s += U[j * lds + k] * X[k][c];
+        T y[QB];
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            if (lane == 0) X[j][c] -= s;
-            __syncwarp();
+        for (int q = 0; q < QB; q++) y[q] = (q * 32 + lane < bs) ? X[q * 32 + lane][c] : T(0);
+#pragma unroll
+        for (int qo = QB - 1; qo >= 0; qo--) {
+            for (int l = 31; l >= 0; l--) {
+                const int j = qo * 32 + l;
+                if (j >= bs) continue;  // warp-uniform
+                const T xj = __shfl_sync(0xffffffffu, y[qo], l);
+#pragma unroll
+                for (int q = 0; q <= qo; q++) {
+                    const int i = q * 32 + lane;
+                    if (i < j) y[q] -= U[i * lds + j] * xj;
+                }
+            }
         }
+#pragma unroll
+        for (int q = 0; q < QB; q++)
+            if (q * 32 + lane < bs) X[q * 32 + lane][c] = y[q];
     }
     __syncthreads();
     for (int idx = threadIdx.x; idx < bs * nr; idx += blockDim.x) {
