@@ -70,7 +70,6 @@ __device__ __forceinline__ void warp_argmax(double &v, int &i)
 // process-wide count of this library's kernel launches (lu2gpu_kernel_launches)
 void count_launch(long k = 1);
 
-// One CTA's published pivot candidate for one leaf column.
 // One CTA's publication for one leaf column.  Every 64-bit word carries the
 // column's 32-bit stamp in its high half and 32 bits of payload in its low
 // half, so a reader validates each word it loads by its stamp (each aligned
