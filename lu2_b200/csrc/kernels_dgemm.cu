@@ -122,7 +122,8 @@ struct GemmCfg {
     static constexpr int MINB = (THREADS <= 128) ? 2 : 1;
 };
 
-// MODE 0: C = C - A * Bt^T (accumulator starts from C, B fragments negated).
+// MODE 0: C = C + A * Bt^T with Bt = -U12^T as the block solve writes it
+// (accumulator starts from C): the trailing update C - L21 U12.
 // MODE 1: C = alpha * A * Bt^T + beta * C (C not read when beta == 0).
 template <int BM, int BN, int WM, int WN, int STAGES, int MODE>
 __global__ void __launch_bounds__(GemmCfg<BM, BN, WM, WN, STAGES>::THREADS, GemmCfg<BM, BN, WM, WN, STAGES>::MINB)
@@ -209,8 +210,8 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, WM, WN, STAGES>::THREADS, Gemm
 #pragma unroll
             for (int nt = 0; nt < NT; nt++) {
                 const double2 v = lds_sw128(sb, warp_n * WN + nt * 8 + pg, chunk);
-                bf[nt][0] = (MODE == 0) ? -v.x : v.x;
-                bf[nt][1] = (MODE == 0) ? -v.y : v.y;
+                bf[nt][0] = v.x;
+                bf[nt][1] = v.y;
             }
 #pragma unroll
             for (int mt = 0; mt < MT; mt++) {

@@ -149,8 +149,8 @@ cudaError_t launch_laswp_scale(float *a, long ld, int k0, int k1, const int *ipi
 // Unit-lower triangular solve of a 32-column strip of the block row, staged
 // in shared memory.  T is consumed in 16-column blocks: each block of T
 // (rows lb..K-1) is first copied to shared memory with coalesced 128-byte row
-// loads, the 16x16 diagonal block is solved column by column by all threads,
-// and the rows below are updated from the staged copy.
+// loads, the 16x16 diagonal block is solved by one lane per column in
+// registers, and the rows below are updated from the staged copy.
 constexpr int TRSM_TW = 32;
 constexpr int TRSM_LDS = TRSM_TW + 1;
 constexpr int TRSM_BK = 16;
@@ -158,10 +158,11 @@ constexpr int TRSM_TLD = TRSM_BK + 1;
 
 // T: the unit lower triangle (strict lower part used), row stride ldt; X: the
 // K x ncols block (row stride ldx) solved in place; bt (optional) receives
-// X^T * bt_scale converted to BT (double, float or bf16).
+// X^T * bt_scale converted to BT (double, float or bf16), negated when bt_neg
+// (the FP64 trailing update reads -U12^T and adds).
 template <typename E, typename BT>
 __global__ void __launch_bounds__(256) trsm_unit_lower_kernel(const E *T, long ldt, E *Xg, long ldx, int K, int ncols,
-                                                              BT *bt, const float *bt_scale)
+                                                              BT *bt, const float *bt_scale, int bt_neg)
 {
     extern __shared__ __align__(16) unsigned char trsm_smem[];
     E *X = reinterpret_cast<E *>(trsm_smem);  // K x TRSM_LDS, then Ts: K x TRSM_TLD
@@ -217,13 +218,13 @@ __global__ void __launch_bounds__(256) trsm_unit_lower_kernel(const E *T, long l
         const int cc = idx / K, r = idx - cc * K;
         if (jbase + cc < ncols) {
             const E v = X[r * TRSM_LDS + cc];
-            bt[(size_t)(jbase + cc) * K + r] = bt_scale ? (BT)(float)(v * (E)sc) : (BT)v;
+            bt[(size_t)(jbase + cc) * K + r] = bt_scale ? (BT)(float)(v * (E)sc) : (BT)(bt_neg ? -v : v);
         }
     }
 }
 
 template <typename E, typename BT>
-static cudaError_t launch_trsm_t(const E *t, long ldt, E *x, long ldx, int K, int ncols, BT *bt, const float *bt_scale,
+static cudaError_t launch_trsm_t(const E *t, long ldt, E *x, long ldx, int K, int ncols, BT *bt, const float *bt_scale, int bt_neg,
                                  cudaStream_t st)
 {
     if (ncols <= 0 || K <= 0) return cudaSuccess;
@@ -236,14 +237,14 @@ static cudaError_t launch_trsm_t(const E *t, long ldt, E *x, long ldx, int K, in
     }
     const int blocks = (ncols + TRSM_TW - 1) / TRSM_TW;
     count_launch();
-    trsm_unit_lower_kernel<E, BT><<<blocks, 256, smem, st>>>(t, ldt, x, ldx, K, ncols, bt, bt_scale);
+    trsm_unit_lower_kernel<E, BT><<<blocks, 256, smem, st>>>(t, ldt, x, ldx, K, ncols, bt, bt_scale, bt_neg);
     return cudaGetLastError();
 }
 
 cudaError_t launch_trsm_unit_lower_tx(const double *t, long ldt, double *x, long ldx, int K, int ncols, double *bt,
                                       cudaStream_t st)
 {
-    return launch_trsm_t<double, double>(t, ldt, x, ldx, K, ncols, bt, nullptr, st);
+    return launch_trsm_t<double, double>(t, ldt, x, ldx, K, ncols, bt, nullptr, 1, st);
 }
 
 cudaError_t launch_trsm_unit_lower(double *a, long ld, int r0, int K, int cs, int ce, double *bt, cudaStream_t st)
@@ -254,13 +255,13 @@ cudaError_t launch_trsm_unit_lower(double *a, long ld, int r0, int K, int cs, in
 cudaError_t launch_trsm_unit_lower_f32(const float *t, long ldt, float *x, long ldx, int K, int ncols, float *bt,
                                        cudaStream_t st)
 {
-    return launch_trsm_t<float, float>(t, ldt, x, ldx, K, ncols, bt, nullptr, st);
+    return launch_trsm_t<float, float>(t, ldt, x, ldx, K, ncols, bt, nullptr, 0, st);
 }
 
 cudaError_t launch_trsm_unit_lower_f32_bf16(const float *t, long ldt, float *x, long ldx, int K, int ncols, void *bt,
                                             const float *bt_scale, cudaStream_t st)
 {
-    return launch_trsm_t<float, __nv_bfloat16>(t, ldt, x, ldx, K, ncols, (__nv_bfloat16 *)bt, bt_scale, st);
+    return launch_trsm_t<float, __nv_bfloat16>(t, ldt, x, ldx, K, ncols, (__nv_bfloat16 *)bt, bt_scale, 0, st);
 }
 
 }  // namespace lu2gpu

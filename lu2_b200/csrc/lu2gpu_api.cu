@@ -1224,7 +1224,8 @@ static int right_part_anyk(lu2gpu_ctx *c, const View &v, int k0, int k1, int cs,
         // L21 (rows k1.., columns k0..k1) into an even-stride buffer, then C -= L21 U12
         CU_TRY(cudaMemcpy2DAsync(lk, ldk * sizeof(double), v.a + (size_t)k1 * v.ld + k0, v.ld * sizeof(double),
                                  (size_t)K * sizeof(double), v.n - k1, cudaMemcpyDeviceToDevice, c->stream));
-        K_TRY(launch_dgemm_general(lk, ldk, c->d_bt, K, v.a + (size_t)k1 * v.ld + cs, v.ld, v.n - k1, ce - cs, K, -1.0,
+        // d_bt holds -U12^T
+        K_TRY(launch_dgemm_general(lk, ldk, c->d_bt, K, v.a + (size_t)k1 * v.ld + cs, v.ld, v.n - k1, ce - cs, K, 1.0,
                                    1.0, c->d_status, c->stream));
     }
     return 0;

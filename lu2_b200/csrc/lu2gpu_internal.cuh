@@ -106,7 +106,7 @@ cudaError_t launch_laswp_scale(float *a, long ld, int k0, int k1, const int *ipi
 
 // In place X := T^{-1} X for the unit lower triangle T = strict lower part of
 // a[r0..r0+K)[r0..r0+K) and X = a[r0..r0+K)[cs..ce); also writes
-// bt[(j-cs)*K + l] = X[l][j] (the transposed block row for the update GEMM).
+// bt[(j-cs)*K + l] = -X[l][j] (the negated transposed block row the update GEMM adds).
 cudaError_t launch_trsm_unit_lower(double *a, long ld, int r0, int K, int cs, int ce, double *bt, cudaStream_t st);
 // The same with the triangle T (row stride ldt) and the K x ncols block X
 // (row stride ldx) given separately; bt may be null.
@@ -119,7 +119,8 @@ cudaError_t launch_trsm_unit_lower_f32(const float *t, long ldt, float *x, long 
 cudaError_t launch_trsm_unit_lower_f32_bf16(const float *t, long ldt, float *x, long ldx, int K, int ncols, void *bt,
                                             const float *bt_scale, cudaStream_t st);
 
-// C[m][n] -= sum_k A[m][k] * Bt[n][k], the trailing update.  A is the
+// C[m][n] += sum_k A[m][k] * Bt[n][k] with Bt = -U12^T (as the block solve
+// writes it), i.e. the trailing update C - L21 U12.  A is the
 // row-major matrix starting at (a_row0, a_col0) of `a` (stride ld, rows < a_rows
 // exist); Bt is (N x K) row-major with stride K.  K % 16 == 0.
 cudaError_t launch_dgemm_update(const double *a, long ld, int a_rows, int a_row0, int a_col0, const double *bt,
