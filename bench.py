@@ -20,6 +20,10 @@ cpu_baseline: the reference compiled from its own sources (oracle/_ref:
          lu2.c/lu2tlib.c/lu2lib.c + OpenBLAS), lumcolumn at N = 8192, all host
          cores.
 
+forms  : BF16-LU + IR and FP8 + GMRES-IR on the diagonally dominant system,
+         the batched form (20,000 small systems), and the host-pointer DGEMM
+         (mydgemm at lu2's update shape, overlapped vs one pass).
+
 --impl reference times that same reference CPU build on a bounded sample
 (N = 8192) of the workload, on rank 0 only.
 Multi-GPU (--gpus N under torchrun): the plain, BF16 and FP8 forms run as
@@ -337,6 +341,48 @@ def fp8_update_bytes(n: int, nb: int) -> float:
     return tot
 
 
+def run_host_dgemm(max_over_ranks, barrier) -> dict:
+    """The board-replacement DGEMM on host pointers (mydgemm, lu2lib.c:2079;
+    gdr_dgemm_ underneath): lu2's trailing-update shape C -= L21 U12 with
+    M = N = 16384, K = 256, row-major, every operand in pinned host memory;
+    overlapped (C in column blocks through three streams) against one pass
+    (LU2GPU_DGEMM_OVERLAP=0: copies in, product, copy out)."""
+    import numpy as np
+    import torch
+
+    import lu2_b200 as L
+
+    m = n = 16384
+    k = 256
+    na = nb = nc = n + 16
+    a = torch.empty((m, na), dtype=torch.float64, pin_memory=True).numpy()
+    b = torch.empty((k, nb), dtype=torch.float64, pin_memory=True).numpy()
+    c = torch.empty((m, nc), dtype=torch.float64, pin_memory=True).numpy()
+    rng = np.random.default_rng(3)
+    a[...] = rng.uniform(-0.5, 0.5, a.shape)
+    b[...] = rng.uniform(-0.5, 0.5, b.shape)
+    c.fill(0.25)
+    flops = 2.0 * m * n * k
+    moved = 8.0 * (m * k + k * n + 2 * m * n)
+    out = {"shape": "row-major C[16384][16384] -= A[16384][256] B[256][16384], pinned host operands",
+           "api": "mydgemm (lu2lib.h) on host pointers"}
+    for label, env in (("overlapped", "1"), ("one_pass", "0")):
+        os.environ["LU2GPU_DGEMM_OVERLAP"] = env
+        ts = []
+        for it in range(4):
+            barrier()
+            t0 = time.perf_counter()
+            L.mydgemm(m, n, k, -1.0, a, na, b, nb, 1.0, c, nc)
+            ts.append(time.perf_counter() - t0)
+        s = max_over_ranks(float(np.median(ts[1:])))
+        out[label] = {"seconds": s, "gflops": flops / s / 1e9, "pcie_gbs": moved / s / 1e9}
+    os.environ.pop("LU2GPU_DGEMM_OVERLAP", None)
+    out["speedup"] = out["one_pass"]["seconds"] / out["overlapped"]["seconds"]
+    log("host dgemm: overlapped %.1f ms, one pass %.1f ms" % (1e3 * out["overlapped"]["seconds"],
+                                                               1e3 * out["one_pass"]["seconds"]))
+    return out
+
+
 def run_fp8(ctx, dev, stream, args, max_over_ranks, world) -> dict:
     """FP8 form: lu2's factorization of an FP32 copy with E4M3 trailing updates
     (per-128x128-tile power-of-two scales, FP32 accumulation), then GMRES-IR
@@ -489,6 +535,7 @@ def main() -> int:
     ap.add_argument("--batch-config", default=None,
                     help="threads,panel_width,ctas_per_sm for --profile-batched (default: autotune)")
     ap.add_argument("--no-fp8", action="store_true", help="skip the FP8 + GMRES-IR measurement")
+    ap.add_argument("--no-host-dgemm", action="store_true", help="skip the host-pointer DGEMM measurement")
     ap.add_argument("--fp8-n", type=int, default=98304)
     ap.add_argument("--fp8-nb", type=int, default=256)
     ap.add_argument("--fp8-check-n", type=int, default=32768)
@@ -688,6 +735,8 @@ def main() -> int:
         forms["batched_fp64"] = run_batched(ctx, dev, stream, args, max_over_ranks, world, rank)
     if not args.no_fp8:
         forms["fp8_gmres_ir"] = run_fp8(ctx, dev, stream, args, max_over_ranks, world)
+    if not args.no_host_dgemm:
+        forms["host_dgemm"] = run_host_dgemm(max_over_ranks, barrier)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

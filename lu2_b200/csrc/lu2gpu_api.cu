@@ -97,6 +97,7 @@ struct lu2gpu_ctx {
     // event per chunk, overlapped with the left-looking start of the factorization
     cudaStream_t h2d_stream = nullptr;
     std::vector<cudaEvent_t> h2d_ev;
+    std::vector<cudaEvent_t> blk_ev;  // blocks of the overlapped host-pointer DGEMM
     // phase timers
     bool timing = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[PH_COUNT];
@@ -230,6 +231,7 @@ extern "C" int lu2gpu_destroy(lu2gpu_ctx *c)
         cudaStreamDestroy(c->h2d_stream);
     }
     for (cudaEvent_t e : c->h2d_ev) cudaEventDestroy(e);
+    for (cudaEvent_t e : c->blk_ev) cudaEventDestroy(e);
     free_mixed(c);
     for (int p = 0; p < PH_COUNT; p++)
         for (auto &e : c->ev[p]) {
@@ -838,6 +840,10 @@ extern "C" int lu2gpu_release(void)
 // Host-pointer column-major DGEMM, the contract of the board library's
 // gdr_dgemm_ (gdrdgemm.c:105-110, 185-186): C = alpha op(A) op(B) + beta C,
 // nota/notb = 1 for no transpose.  Computed as the row-major C^T = op(B)^T op(A)^T.
+static int host_dgemm_colmajor_overlap(lu2gpu_ctx *c, int nota, int notb, int m, int n, int k, double alpha,
+                                       const double *A, int lda, const double *B, int ldb, double beta, double *C,
+                                       int ldc, int jb);
+
 static int host_dgemm_colmajor(int nota, int notb, int m, int n, int k, double alpha, const double *A, int lda,
                                const double *B, int ldb, double beta, double *C, int ldc)
 {
@@ -849,6 +855,17 @@ static int host_dgemm_colmajor(int nota, int notb, int m, int n, int k, double a
     }
     if (m == 0 || n == 0) return 0;
     DeviceGuard g(c->device);
+    if (k > 0 && A && B) {
+        // C in pinned host memory and at least two blocks of ~16 MB: overlapped
+        cudaPointerAttributes pa{};
+        const bool pinned = cudaPointerGetAttributes(&pa, C) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+        cudaGetLastError();
+        const char *ov = getenv("LU2GPU_DGEMM_OVERLAP");
+        long jb = (16L << 20) / ((long)m * (long)sizeof(double));
+        if (jb < 16) jb = 16;
+        if (pinned && !(ov && atoi(ov) == 0) && 2 * jb <= n)
+            return host_dgemm_colmajor_overlap(c, nota, notb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, (int)jb);
+    }
     int rc = begin_status(c);
     if (rc) return rc;
     const int kk = k > 0 ? k : 1;
@@ -895,6 +912,87 @@ static int host_dgemm_colmajor(int nota, int notb, int m, int n, int k, double a
     K_TRY(launch_dgemm_general(X, ldk, Y, ldk, Cd, ldcd, n, m, kk, alpha, beta, c->d_status, c->stream));
     CU_TRY(cudaMemcpy2DAsync(C, (size_t)ldc * sizeof(double), Cd, ldcd * sizeof(double), (size_t)m * sizeof(double),
                              n, cudaMemcpyDeviceToHost, c->stream));
+    return end_status(c, "gdr_dgemm_");
+}
+
+static int ensure_events(std::vector<cudaEvent_t> &v, size_t count)
+{
+    while (v.size() < count) {
+        cudaEvent_t e;
+        CU_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        v.push_back(e);
+    }
+    return 0;
+}
+
+// The same product with C in pinned (or registered) host memory, overlapped
+// as the board library's "-ovl" build did (Makefile.mgv:29): op(A) goes to the
+// device first; then blocks of jb columns of C (with their columns of op(B))
+// go in on one stream, are multiplied on the context's stream and come back on
+// a third, so block b+1's copy in, block b's product and block b-1's copy out
+// run together (PCIe carries both directions at once).  Each block's product
+// is the one-pass product's for those columns: bit-identical results.
+static int host_dgemm_colmajor_overlap(lu2gpu_ctx *c, int nota, int notb, int m, int n, int k, double alpha,
+                                       const double *A, int lda, const double *B, int ldb, double beta, double *C,
+                                       int ldc, int jb)
+{
+    int rc = begin_status(c);
+    if (rc) return rc;
+    const long ldk = (k + 1) & ~1L, ldcd = (m + 1) & ~1L, ldtx = (jb + 1) & ~1L, ldty = (m + 1) & ~1L;
+    double *X, *Y, *T, *Cd;
+    if ((rc = stage(c, 0, (size_t)n * ldk, &X)) || (rc = stage(c, 1, (size_t)m * ldk, &Y)) ||
+        (rc = stage(c, 2, (size_t)n * ldcd, &Cd)) ||
+        (rc = stage(c, 3, (size_t)k * (ldtx > ldty ? ldtx : ldty), &T)))
+        return rc;
+    if (!c->h2d_stream) CU_TRY(cudaStreamCreateWithFlags(&c->h2d_stream, cudaStreamNonBlocking));
+    if (!c->copy_stream) {
+        CU_TRY(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+        CU_TRY(cudaEventCreateWithFlags(&c->copy_ev, cudaEventDisableTiming));
+    }
+    const int nblk = (n + jb - 1) / jb;
+    if ((rc = ensure_events(c->h2d_ev, (size_t)nblk + 1)) || (rc = ensure_events(c->blk_ev, (size_t)nblk + 1)))
+        return rc;
+    // op(A)[i][q] on the context's stream
+    if (!nota) {
+        CU_TRY(cudaMemcpy2DAsync(Y, ldk * sizeof(double), A, (size_t)lda * sizeof(double), (size_t)k * sizeof(double),
+                                 m, cudaMemcpyHostToDevice, c->stream));
+    } else {
+        CU_TRY(cudaMemcpy2DAsync(T, ldty * sizeof(double), A, (size_t)lda * sizeof(double), (size_t)m * sizeof(double),
+                                 k, cudaMemcpyHostToDevice, c->stream));
+        K_TRY(launch_transpose(T, ldty, Y, ldk, k, m, c->stream));
+    }
+    // the block copies start after everything before them on the context's stream
+    CU_TRY(cudaEventRecord(c->h2d_ev[nblk], c->stream));
+    CU_TRY(cudaStreamWaitEvent(c->h2d_stream, c->h2d_ev[nblk], 0));
+    for (int b = 0; b < nblk; b++) {
+        const int j0 = b * jb, nj = (n - j0) < jb ? n - j0 : jb;
+        // op(B)^T rows j0..j0+nj-1: notb -> B[q + j*ldb]; else B[j + q*ldb] (transposed via T)
+        if (notb) {
+            CU_TRY(cudaMemcpy2DAsync(X + (size_t)j0 * ldk, ldk * sizeof(double), B + (size_t)j0 * ldb,
+                                     (size_t)ldb * sizeof(double), (size_t)k * sizeof(double), nj,
+                                     cudaMemcpyHostToDevice, c->h2d_stream));
+        } else {
+            CU_TRY(cudaMemcpy2DAsync(T, ldtx * sizeof(double), B + j0, (size_t)ldb * sizeof(double),
+                                     (size_t)nj * sizeof(double), k, cudaMemcpyHostToDevice, c->h2d_stream));
+            K_TRY(launch_transpose(T, ldtx, X + (size_t)j0 * ldk, ldk, k, nj, c->h2d_stream));
+        }
+        if (beta != 0.0)
+            CU_TRY(cudaMemcpy2DAsync(Cd + (size_t)j0 * ldcd, ldcd * sizeof(double), C + (size_t)j0 * ldc,
+                                     (size_t)ldc * sizeof(double), (size_t)m * sizeof(double), nj,
+                                     cudaMemcpyHostToDevice, c->h2d_stream));
+        CU_TRY(cudaEventRecord(c->h2d_ev[b], c->h2d_stream));
+        CU_TRY(cudaStreamWaitEvent(c->stream, c->h2d_ev[b], 0));
+        K_TRY(launch_dgemm_general(X + (size_t)j0 * ldk, ldk, Y, ldk, Cd + (size_t)j0 * ldcd, ldcd, nj, m, k, alpha,
+                                   beta, c->d_status, c->stream));
+        CU_TRY(cudaEventRecord(c->blk_ev[b], c->stream));
+        CU_TRY(cudaStreamWaitEvent(c->copy_stream, c->blk_ev[b], 0));
+        CU_TRY(cudaMemcpy2DAsync(C + (size_t)j0 * ldc, (size_t)ldc * sizeof(double), Cd + (size_t)j0 * ldcd,
+                                 ldcd * sizeof(double), (size_t)m * sizeof(double), nj, cudaMemcpyDeviceToHost,
+                                 c->copy_stream));
+    }
+    // the last copy out precedes what follows on the context's stream
+    CU_TRY(cudaEventRecord(c->blk_ev[nblk], c->copy_stream));
+    CU_TRY(cudaStreamWaitEvent(c->stream, c->blk_ev[nblk], 0));
     return end_status(c, "gdr_dgemm_");
 }
 

@@ -111,3 +111,59 @@ def test_device_dgemm(ctx):
     ctx.dgemm(m, n, k, 2.0, a, k, b, n, 1.0, c, n)
     an, bn = a.cpu().numpy(), b.cpu().numpy()
     assert np.all(np.abs(c.cpu().numpy() - ref) <= 2 * bound(an, bn, k, ref))
+
+
+def _pinned_like(x):
+    """a pinned-host numpy array with x's contents and memory order"""
+    import torch
+
+    t = torch.empty(x.size, dtype=torch.float64, pin_memory=True)
+    order = "F" if (x.flags.f_contiguous and not x.flags.c_contiguous) else "C"
+    out = t.numpy().reshape(x.shape, order=order)
+    out[...] = x
+    return out, t
+
+
+@pytest.mark.parametrize("nota,notb", [(1, 1), (0, 1), (1, 0), (0, 0)])
+def test_gdr_dgemm_pinned_overlap_is_bit_identical(nota, notb):
+    """C in pinned host memory takes the overlapped path (blocks of C's
+    columns copied in, multiplied and copied out on three streams); it gives
+    the one-pass (pageable) path's result bit for bit."""
+    rng = np.random.default_rng(31 + 2 * nota + notb)
+    m, n, k = 2048, 2600, 96  # ~16 MB blocks of 1024 columns: 3 blocks, the last ragged
+    lda, ldb, ldc = (m if nota else k) + 2, (k if notb else n) + 1, m + 3
+    A = np.asfortranarray(rng.uniform(-1, 1, (lda, k if nota else m)))
+    B = np.asfortranarray(rng.uniform(-1, 1, (ldb, n if notb else k)))
+    C0 = np.asfortranarray(rng.uniform(-1, 1, (ldc, n)))
+    Cpg = C0.copy(order="F")
+    assert L.gdr_dgemm_(nota, notb, m, n, k, 1.5, -0.25, lda, ldb, ldc, A, B, Cpg) == 1
+    Cpin, keep = _pinned_like(C0)
+    assert Cpin.flags.f_contiguous
+    assert L.gdr_dgemm_(nota, notb, m, n, k, 1.5, -0.25, lda, ldb, ldc, A, B, Cpin) == 1
+    assert np.array_equal(Cpin, Cpg)
+    opA = A[:m, :k] if nota else A[:k, :m].T
+    opB = B[:k, :n] if notb else B[:n, :k].T
+    ref = 1.5 * opA @ opB - 0.25 * C0[:m, :n]
+    assert np.all(np.abs(Cpin[:m, :n] - ref) <= bound(opA, opB, k, ref))
+
+
+def test_mydgemm_pinned_overlap_lu2_shape():
+    """lu2's trailing update through mydgemm (C -= L21 U12, row-major, k = nb)
+    on pinned host buffers: overlapped, bit-identical to the pageable call,
+    and beta = 0 never reads C."""
+    rng = np.random.default_rng(5)
+    m, n, k = 3000, 2100, 256
+    na, nb, nc = k + 16, n + 16, n + 16
+    a = rng.uniform(-1, 1, (m, na))
+    b = rng.uniform(-1, 1, (k, nb))
+    c0 = rng.uniform(-1, 1, (m, nc))
+    cpg = c0.copy()
+    L.mydgemm(m, n, k, -1.0, a, na, b, nb, 1.0, cpg, nc)
+    cpin, keep = _pinned_like(c0)
+    L.mydgemm(m, n, k, -1.0, a, na, b, nb, 1.0, cpin, nc)
+    assert np.array_equal(cpin, cpg)
+    cpin[:, :n] = np.nan
+    L.mydgemm(m, n, k, 1.0, a, na, b, nb, 0.0, cpin, nc)
+    ref = a[:, :k] @ b[:, :n]
+    assert np.all(np.abs(cpin[:, :n] - ref) <= bound(a[:, :k], b[:, :n], k, ref))
+    assert np.array_equal(cpin[:, n:], c0[:, n:])
