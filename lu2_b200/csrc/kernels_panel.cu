@@ -200,7 +200,24 @@ __global__ void __launch_bounds__(256) trsm_unit_lower_kernel(const E *T, long l
         E xb[TRSM_BK];
 #pragma unroll
         for (int l = 0; l < TRSM_BK; l++) xb[l] = (l < bk) ? X[(lb + l) * TRSM_LDS + col] : 0.0;
-        for (int r = lb + bk + rg; r < K; r += 8) {
+        // four rows at a time: independent dot-product chains overlap
+        int r = lb + bk + rg;
+        for (; r + 24 < K; r += 32) {
+            const E *Tr = Ts + (r - lb) * TRSM_TLD;
+            E s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+#pragma unroll
+            for (int l = 0; l < TRSM_BK; l++) {
+                s0 += Tr[l] * xb[l];
+                s1 += Tr[8 * TRSM_TLD + l] * xb[l];
+                s2 += Tr[16 * TRSM_TLD + l] * xb[l];
+                s3 += Tr[24 * TRSM_TLD + l] * xb[l];
+            }
+            X[r * TRSM_LDS + col] -= s0;
+            X[(r + 8) * TRSM_LDS + col] -= s1;
+            X[(r + 16) * TRSM_LDS + col] -= s2;
+            X[(r + 24) * TRSM_LDS + col] -= s3;
+        }
+        for (; r < K; r += 8) {
             const E *Tr = Ts + (r - lb) * TRSM_TLD;
             E s = 0;
 #pragma unroll
