@@ -95,8 +95,21 @@ __global__ void __launch_bounds__(SWAP_THREADS) laswp_scale_kernel(T *a, long ld
     for (int chunk = blockIdx.x; chunk < nchunk; chunk += gridDim.x) {
         const int j = cs + chunk * SWAP_COLS + c;
         const bool jok = j < ce;
-        for (int s = tid / SWAP_COLS; s < nslot; s += SWAP_THREADS / SWAP_COLS)
-            V[s * SWAP_COLS + c] = jok ? a[(size_t)rowof[cur[s]] * ld + j] : 0.0;
+        // gather with GATHER_U loads in flight per thread
+        constexpr int STEP = SWAP_THREADS / SWAP_COLS, GATHER_U = 8;
+        for (int s0 = tid / SWAP_COLS; s0 < nslot; s0 += GATHER_U * STEP) {
+            T v[GATHER_U];
+#pragma unroll
+            for (int u = 0; u < GATHER_U; u++) {
+                const int s = s0 + u * STEP;
+                v[u] = (jok && s < nslot) ? a[(size_t)rowof[cur[s]] * ld + j] : T(0);
+            }
+#pragma unroll
+            for (int u = 0; u < GATHER_U; u++) {
+                const int s = s0 + u * STEP;
+                if (s < nslot) V[s * SWAP_COLS + c] = v[u];
+            }
+        }
         __syncthreads();
         if (jok) {
             for (int s = tid / SWAP_COLS; s < nslot; s += SWAP_THREADS / SWAP_COLS) {
