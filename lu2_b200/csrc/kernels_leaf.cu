@@ -95,9 +95,22 @@ __global__ void __launch_bounds__(LEAF_THREADS) leaf_kernel(LeafParams<T> P)
     const int re = min(P.n, rb + rpc);
     const int nr = max(0, re - rb);
 
-    for (int idx = tid; idx < nr * LEAF_W; idx += LEAF_THREADS) {
-        const int lr = idx / LEAF_W, j = idx - lr * LEAF_W;
-        slab[lr * LEAF_LDS + j] = (j < w) ? P.a[(size_t)(rb + lr) * P.ld + c0 + j] : 0.0;
+    // the slab, with SLAB_U loads in flight per thread
+    constexpr int SLAB_U = 8;
+    for (int idx0 = tid; idx0 < nr * LEAF_W; idx0 += SLAB_U * LEAF_THREADS) {
+        T v[SLAB_U];
+#pragma unroll
+        for (int u = 0; u < SLAB_U; u++) {
+            const int idx = idx0 + u * LEAF_THREADS;
+            const int lr = idx / LEAF_W, j = idx - lr * LEAF_W;
+            v[u] = (idx < nr * LEAF_W && j < w) ? P.a[(size_t)(rb + lr) * P.ld + c0 + j] : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < SLAB_U; u++) {
+            const int idx = idx0 + u * LEAF_THREADS;
+            const int lr = idx / LEAF_W, j = idx - lr * LEAF_W;
+            if (idx < nr * LEAF_W) slab[lr * LEAF_LDS + j] = v[u];
+        }
     }
     if (tid == 0) s_fail = 0;
     __syncthreads();
