@@ -35,13 +35,23 @@ __device__ __forceinline__ void batch_block_argmax(double &v, int &i, double *s_
     __syncthreads();    // partials read before the next reduction writes them
 }
 
+constexpr int BATCH_LOAD_U = 4;  // global loads a thread keeps in flight when staging
+
 // whole system in shared memory: S (n x nc, stride nc)
 __device__ void batch_solve_smem(double *A, long ld, int n, int nrhs, double *S, int *info, double *s_v, int *s_i)
 {
     const int nc = n + nrhs, T = blockDim.x, tid = threadIdx.x;
-    for (int idx = tid; idx < n * nc; idx += T) {
-        const int r = idx / nc, c = idx - r * nc;
-        S[idx] = A[(size_t)r * ld + c];
+    // BATCH_LOAD_U loads in flight per thread
+    for (int idx0 = tid; idx0 < n * nc; idx0 += BATCH_LOAD_U * T) {
+        double v[BATCH_LOAD_U];
+#pragma unroll
+        for (int u = 0; u < BATCH_LOAD_U; u++) {
+            const int idx = idx0 + u * T, r = idx / nc, c = idx - r * nc;
+            v[u] = (idx < n * nc) ? A[(size_t)r * ld + c] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < BATCH_LOAD_U; u++)
+            if (idx0 + u * T < n * nc) S[idx0 + u * T] = v[u];
     }
     __syncthreads();
     int first_zero = 0;
@@ -116,9 +126,18 @@ __device__ void batch_solve_blocked(double *A, long ld, int n, int nrhs, int pw,
     for (int k0 = 0; k0 < n; k0 += pw) {
         const int w = min(pw, n - k0), rows = n - k0;
         // panel rows k0..n-1, columns k0..k0+w-1 -> P (rows x ps)
-        for (int idx = tid; idx < rows * w; idx += T) {
-            const int r = idx / w, c = idx - r * w;
-            P[r * ps + c] = A[(size_t)(k0 + r) * ld + k0 + c];
+        for (int idx0 = tid; idx0 < rows * w; idx0 += BATCH_LOAD_U * T) {
+            double v[BATCH_LOAD_U];
+#pragma unroll
+            for (int u = 0; u < BATCH_LOAD_U; u++) {
+                const int idx = idx0 + u * T, r = idx / w, c = idx - r * w;
+                v[u] = (idx < rows * w) ? A[(size_t)(k0 + r) * ld + k0 + c] : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < BATCH_LOAD_U; u++) {
+                const int idx = idx0 + u * T, r = idx / w, c = idx - r * w;
+                if (idx < rows * w) P[r * ps + c] = v[u];
+            }
         }
         __syncthreads();
         for (int c = 0; c < w; c++) {
