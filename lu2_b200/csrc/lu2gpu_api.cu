@@ -936,6 +936,9 @@ static int host_dgemm_colmajor_overlap(lu2gpu_ctx *c, int nota, int notb, int m,
                                        const double *A, int lda, const double *B, int ldb, double beta, double *C,
                                        int ldc, int jb)
 {
+    // nothing of an earlier call (one that may have failed half way) still in flight
+    if (c->copy_stream) CU_TRY(cudaStreamSynchronize(c->copy_stream));
+    if (c->h2d_stream) CU_TRY(cudaStreamSynchronize(c->h2d_stream));
     int rc = begin_status(c);
     if (rc) return rc;
     const long ldk = (k + 1) & ~1L, ldcd = (m + 1) & ~1L, ldtx = (jb + 1) & ~1L, ldty = (m + 1) & ~1L;
@@ -1193,7 +1196,9 @@ static int lumcolumn_host(int n, double *a, double *b, int m, int *pv)
     cudaPointerAttributes pa{};
     const bool pinned = cudaPointerGetAttributes(&pa, a) == cudaSuccess && pa.type == cudaMemoryTypeHost;
     cudaGetLastError();
-    if (c->copy_stream) CU_TRY(cudaStreamSynchronize(c->copy_stream));  // nothing of an earlier call in flight
+    // nothing of an earlier call (one that may have failed half way) still in flight
+    if (c->copy_stream) CU_TRY(cudaStreamSynchronize(c->copy_stream));
+    if (c->h2d_stream) CU_TRY(cudaStreamSynchronize(c->h2d_stream));
     if (pinned && !c->copy_stream) {
         CU_TRY(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
         CU_TRY(cudaEventCreateWithFlags(&c->copy_ev, cudaEventDisableTiming));
