@@ -70,7 +70,11 @@ extern "C" {
  * a receives the factors (y in column n); pv[0..m) the last panel's pivot
  * rows, as the reference leaves them.  awork and recursive are accepted and
  * unused.  Pivot mode: LU2GPU_PIVOT_PARTIAL unless lu2gpu_set_pivot_mode()
- * or the environment variable LU2GPU_PIVOT=ref selects the reference's. */
+ * or the environment variable LU2GPU_PIVOT=ref selects the reference's.
+ * With a in pinned (or registered) host memory the copies overlap the
+ * factorization: a goes to the GPU in column chunks while the first panels
+ * are factored left-looking, and finished factor blocks come back while the
+ * rest is factored; the result is bit-identical to the pageable path's. */
 void lumcolumn(int n, double *a, double *b, int m, double *awork, int *pv, int recursive);
 
 /* lu2.c's per-panel steps on the host matrix a[n][n+16] (each stages the
@@ -96,7 +100,12 @@ void cm_column_decomposition_recursive(int n, double *a, int m, int *pv, int i);
 void cm_column_decomposition(int n, double *a, int m, int *pv, int i);
 void cm_process_right_part(int n, double *a, int m, int *pv, int i, int iend);
 
-/* lu2lib.h:9-19, lu2lib.c:2079-2136: row-major C = alpha*A*B + beta*C. */
+/* lu2lib.h:9-19, lu2lib.c:2079-2136: row-major C = alpha*A*B + beta*C.
+ * This and the board-library DGEMMs below take host pointers; with C in
+ * pinned host memory (and at least two ~16 MB column blocks of it) the copies
+ * in, the products and the copies out of C's column blocks overlap on three
+ * streams, bit-identical to the one-pass path (LU2GPU_DGEMM_OVERLAP=0 forces
+ * that path). */
 void mydgemm(int m, int n, int k, double alpha, double *a, int na, double *b, int nb, double beta, double *c,
              int nc);
 
@@ -157,7 +166,13 @@ int lu2gpu_set_stream(lu2gpu_ctx *ctx, void *stream);
  * dimension lda, even; a 16-byte aligned) in place with block size nb (a
  * multiple of 16): recursive panels down to 16 columns, lu2's storage.  The
  * right-hand-side columns come out forward-transformed (y).  ipiv (device,
- * n ints, may be NULL) receives the pivot sequence.  Synchronous. */
+ * n ints, may be NULL) receives the pivot sequence.  Synchronous.
+ * From four panels up, the next panel is factored on a second stream of the
+ * context (highest priority) while the rest of the trailing update runs
+ * (the lookahead of lu2_mpi.c:3643-3847); every element sees the same
+ * operations in the same order as in the serial schedule, so the result is
+ * bit-identical.  LU2GPU_LOOKAHEAD=0 in the environment, or phase timing,
+ * selects the serial schedule. */
 int lu2gpu_factor(lu2gpu_ctx *ctx, int n, int nrhs, double *a, long lda, int nb, int pivot_mode, int *ipiv);
 
 /* x = U'^{-1} y with the unit upper factor of a (lu2.c:110-116); y is the
