@@ -532,6 +532,8 @@ def main() -> int:
                     help="profiling run for ncu: one FP8-LU + GMRES-IR solve of the diagonally dominant system")
     ap.add_argument("--profile-batched", action="store_true",
                     help="profiling run for ncu: one FP64 batched solve of the batch-count systems")
+    ap.add_argument("--batch-ir", action="store_true",
+                    help="--profile-batched in the FP32-LU + FP64 IR mode")
     ap.add_argument("--batch-config", default=None,
                     help="threads,panel_width,ctas_per_sm for --profile-batched (default: autotune)")
     ap.add_argument("--no-fp8", action="store_true", help="skip the FP8 + GMRES-IR measurement")
@@ -586,6 +588,8 @@ def main() -> int:
         b = L.Batch(ctx, n_b, r_b)
         b.generate_seeds(1 + np.arange(args.batch_count))
         b.snapshot()  # the original systems, for the residuals
+        if args.batch_ir:
+            b.set_mode(L.BATCH_FP32_IR, 10)
         if args.batch_config:
             t_, pw_, g_ = (int(v) for v in args.batch_config.split(","))
             b.set_config(t_, pw_, g_)

@@ -81,23 +81,24 @@ __device__ void ir_factor_smem(float *F, int n, int *piv, int *first_zero, doubl
 }
 
 // FP32 factorization of F (n x n, stride n) in global memory, panel of pw
-// columns staged in shared memory (P: rows x pw, U: pw x 64)
+// columns staged in shared memory (P: rows x (pw+1), U: pw x 64)
 __device__ void ir_factor_blocked(float *F, int n, int pw, float *P, float *U, int *piv, float *dinv,
                                   int *first_zero, double *s_v, int *s_i)
 {
     const int T = blockDim.x, tid = threadIdx.x;
+    const int ps = pw + 1;  // odd panel row stride: a column's rows fall in distinct banks
     for (int k0 = 0; k0 < n; k0 += pw) {
         const int w = min(pw, n - k0), rows = n - k0;
         for (int idx = tid; idx < rows * w; idx += T) {
             const int r = idx / w, c = idx - r * w;
-            P[r * pw + c] = F[(size_t)(k0 + r) * n + k0 + c];
+            P[r * ps + c] = F[(size_t)(k0 + r) * n + k0 + c];
         }
         __syncthreads();
         for (int c = 0; c < w; c++) {
             double v = -1.0;
             int p = INT_MAX;
             for (int r = c + tid; r < rows; r += T) {
-                const double a = fabsf(P[r * pw + c]);
+                const double a = fabsf(P[r * ps + c]);
                 if (a > v) {
                     v = a;
                     p = r;
@@ -108,31 +109,31 @@ __device__ void ir_factor_blocked(float *F, int n, int pw, float *P, float *U, i
             if (tid == 0) piv[k0 + c] = k0 + p;
             if (p != c)
                 for (int j = tid; j < w; j += T) {
-                    const float t = P[c * pw + j];
-                    P[c * pw + j] = P[p * pw + j];
-                    P[p * pw + j] = t;
+                    const float t = P[c * ps + j];
+                    P[c * ps + j] = P[p * ps + j];
+                    P[p * ps + j] = t;
                 }
             __syncthreads();
-            const float d = P[c * pw + c];
+            const float d = P[c * ps + c];
             const bool zero = (d == 0.f);
             if (zero && !*first_zero && tid == 0) *first_zero = k0 + c + 1;
             const float inv = zero ? 1.f : 1.f / d;
             if (tid == 0) dinv[c] = inv;
             if (!zero)
-                for (int j = c + 1 + tid; j < w; j += T) P[c * pw + j] *= inv;
+                for (int j = c + 1 + tid; j < w; j += T) P[c * ps + j] *= inv;
             __syncthreads();
             if (!zero) {
                 const int wj = w - c - 1, hr = rows - c - 1;
                 for (int idx = tid; idx < hr * wj; idx += T) {
                     const int r = c + 1 + idx / wj, j = c + 1 + idx % wj;
-                    P[r * pw + j] -= P[r * pw + c] * P[c * pw + j];
+                    P[r * ps + j] -= P[r * ps + c] * P[c * ps + j];
                 }
             }
             __syncthreads();
         }
         for (int idx = tid; idx < rows * w; idx += T) {
             const int r = idx / w, c = idx - r * w;
-            F[(size_t)(k0 + r) * n + k0 + c] = P[r * pw + c];
+            F[(size_t)(k0 + r) * n + k0 + c] = P[r * ps + c];
         }
         // exchanges of the earlier panels' columns (full-width rows), one thread per column
         for (int j = tid; j < k0; j += T)
@@ -164,7 +165,7 @@ __device__ void ir_factor_blocked(float *F, int n, int pw, float *P, float *U, i
             }
             for (int r = 0; r < w; r++) {
                 float s = x[r];
-                for (int l = 0; l < r; l++) s -= P[r * pw + l] * x[l];
+                for (int l = 0; l < r; l++) s -= P[r * ps + l] * x[l];
                 x[r] = s * dinv[r];
             }
             for (int c = 0; c < w; c++) F[(size_t)(k0 + c) * n + j] = x[c];
@@ -186,7 +187,7 @@ __device__ void ir_factor_blocked(float *F, int n, int pw, float *P, float *U, i
                     float av[4], bv[4];
 #pragma unroll
                     for (int i = 0; i < 4; i++) {
-                        av[i] = (rb + i < h) ? P[(w + rb + i) * pw + l] : 0.f;
+                        av[i] = (rb + i < h) ? P[(w + rb + i) * ps + l] : 0.f;
                         bv[i] = U[l * 64 + tx * 4 + i];
                     }
 #pragma unroll
@@ -362,7 +363,7 @@ __global__ void batch_ir_kernel(double *data, const BatchSys *sys, const long lo
         double *R = X + (size_t)n * r;
         const bool in_smem = (long)n * n + (long)n * r <= smem_floats;
         float *F = in_smem ? ism : Fg;
-        float *V = in_smem ? ism + (size_t)n * n : ism + (size_t)n * pw + (size_t)pw * 64;
+        float *V = in_smem ? ism + (size_t)n * n : ism + (size_t)n * (pw + 1) + (size_t)pw * 64;
         if (tid == 0) s_zero = 0;
         for (int idx = tid; idx < n * n; idx += T) {
             const int i = idx / n, j = idx - i * n;
@@ -372,7 +373,7 @@ __global__ void batch_ir_kernel(double *data, const BatchSys *sys, const long lo
         if (in_smem)
             ir_factor_smem(F, n, piv, &s_zero, s_v, s_i);
         else
-            ir_factor_blocked(F, n, pw, ism, ism + (size_t)n * pw, piv, s_dinv, &s_zero, s_v, s_i);
+            ir_factor_blocked(F, n, pw, ism, ism + (size_t)n * (pw + 1), piv, s_dinv, &s_zero, s_v, s_i);
         __syncthreads();
         int it = 0;
         if (s_zero == 0) {
@@ -420,7 +421,7 @@ long batch_ir_smem_floats(const BatchSys *sys, int count, int pw, long floor_flo
 {
     long need = floor_floats;
     for (int i = 0; i < count; i++) {
-        const long b = (long)sys[i].n * pw + (long)pw * 64 + (long)sys[i].n * sys[i].nrhs;
+        const long b = (long)sys[i].n * (pw + 1) + (long)pw * 64 + (long)sys[i].n * sys[i].nrhs;
         if (b > need) need = b;
     }
     return need;

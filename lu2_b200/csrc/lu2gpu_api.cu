@@ -1980,8 +1980,10 @@ static void batch_drop_graph(lu2gpu_batch *b)
 static int batch_configure(lu2gpu_batch *b, int threads, int pw, int ctas_per_sm)
 {
     if (b->mode == LU2GPU_BATCH_FP32_IR) {
-        // the FP32 variant keeps as many systems as fit entirely in shared memory
-        const long floor_floats = (long)(BATCH_SMEM_MAX / sizeof(float)) / (ctas_per_sm > 1 ? 2 : 1);
+        // the FP32 variant keeps as many systems as fit entirely in shared memory;
+        // for two CTAs per SM each keeps 8 KB clear for the kernel's static shared memory
+        const long floor_floats =
+            (long)((ctas_per_sm > 1 ? BATCH_SMEM_MAX / 2 - 8192 : BATCH_SMEM_MAX) / sizeof(float));
         const long sf = batch_ir_smem_floats(b->sys.data(), b->count, pw, floor_floats);
         if ((size_t)sf * sizeof(float) > BATCH_SMEM_MAX) {
             set_error("batch: panel width %d needs %ld bytes of shared memory for n=%d (limit %zu)", pw,
