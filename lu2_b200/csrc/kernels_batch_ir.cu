@@ -39,14 +39,14 @@ __device__ __forceinline__ void ir_block_argmax(double &v, int &i, double *s_v, 
 }
 
 // FP32 factorization of F (n x n, stride n) held in shared memory
-__device__ void ir_factor_smem(float *F, int n, int *piv, int *first_zero, double *s_v, int *s_i)
+__device__ void ir_factor_smem(float *F, int n, int fs, int *piv, int *first_zero, double *s_v, int *s_i)
 {
     const int T = blockDim.x, tid = threadIdx.x;
     for (int k = 0; k < n; k++) {
         double v = -1.0;
         int p = INT_MAX;
         for (int r = k + tid; r < n; r += T) {
-            const double a = fabsf(F[r * n + k]);
+            const double a = fabsf(F[r * fs + k]);
             if (a > v) {
                 v = a;
                 p = r;
@@ -57,24 +57,24 @@ __device__ void ir_factor_smem(float *F, int n, int *piv, int *first_zero, doubl
         if (tid == 0) piv[k] = p;
         if (p != k)
             for (int c = tid; c < n; c += T) {
-                const float t = F[k * n + c];
-                F[k * n + c] = F[p * n + c];
-                F[p * n + c] = t;
+                const float t = F[k * fs + c];
+                F[k * fs + c] = F[p * fs + c];
+                F[p * fs + c] = t;
             }
         __syncthreads();
-        const float d = F[k * n + k];
+        const float d = F[k * fs + k];
         if (d == 0.f) {
             if (!*first_zero && tid == 0) *first_zero = k + 1;
             __syncthreads();
             continue;
         }
         const float inv = 1.f / d;
-        for (int c = k + 1 + tid; c < n; c += T) F[k * n + c] *= inv;
+        for (int c = k + 1 + tid; c < n; c += T) F[k * fs + c] *= inv;
         __syncthreads();
         const int w = n - k - 1;
         for (int idx = tid; idx < w * w; idx += T) {
             const int r = k + 1 + idx / w, c = k + 1 + idx % w;
-            F[r * n + c] -= F[r * n + k] * F[k * n + c];
+            F[r * fs + c] -= F[r * fs + k] * F[k * fs + c];
         }
         __syncthreads();
     }
@@ -212,7 +212,7 @@ __device__ void ir_factor_blocked(float *F, int n, int pw, float *P, float *U, i
 // V (n x r, row-major, shared memory) = U'^{-1} L'^{-1} P V with the FP32 factors F
 // (stride n, shared or global memory); blocks of 32 rows: one warp solves the
 // diagonal block, every thread updates the rows beyond it
-__device__ void ir_solve(const float *F, int n, const int *piv, float *V, int r)
+__device__ void ir_solve(const float *F, int n, int fs, const int *piv, float *V, int r)
 {
     const int T = blockDim.x, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     for (int q = tid; q < r; q += T)
@@ -233,16 +233,16 @@ __device__ void ir_solve(const float *F, int n, const int *piv, float *V, int r)
                 float v = lane < bw ? V[(b0 + lane) * r + q] : 0.f;
                 for (int k = 0; k < bw; k++) {
                     float yk = __shfl_sync(0xffffffffu, v, k);
-                    yk /= F[(size_t)(b0 + k) * n + b0 + k];
+                    yk /= F[(size_t)(b0 + k) * fs + b0 + k];
                     if (lane == k) v = yk;
-                    if (lane > k && lane < bw) v -= F[(size_t)(b0 + lane) * n + b0 + k] * yk;
+                    if (lane > k && lane < bw) v -= F[(size_t)(b0 + lane) * fs + b0 + k] * yk;
                 }
                 if (lane < bw) V[(b0 + lane) * r + q] = v;
             }
         __syncthreads();
         for (int idx = tid; idx < (n - b0 - bw) * r; idx += T) {
             const int i = b0 + bw + idx / r, q = idx % r;
-            const float *row = F + (size_t)i * n + b0;
+            const float *row = F + (size_t)i * fs + b0;
             float s = 0.f;
             for (int k = 0; k < bw; k++) s = fmaf(row[k], V[(b0 + k) * r + q], s);
             V[i * r + q] -= s;
@@ -257,14 +257,14 @@ __device__ void ir_solve(const float *F, int n, const int *piv, float *V, int r)
                 float v = lane < bw ? V[(b0 + lane) * r + q] : 0.f;
                 for (int k = bw - 1; k >= 0; k--) {
                     const float xk = __shfl_sync(0xffffffffu, v, k);
-                    if (lane < k) v -= F[(size_t)(b0 + lane) * n + b0 + k] * xk;
+                    if (lane < k) v -= F[(size_t)(b0 + lane) * fs + b0 + k] * xk;
                 }
                 if (lane < bw) V[(b0 + lane) * r + q] = v;
             }
         __syncthreads();
         for (int idx = tid; idx < b0 * r; idx += T) {
             const int i = idx / r, q = idx % r;
-            const float *row = F + (size_t)i * n + b0;
+            const float *row = F + (size_t)i * fs + b0;
             float s = 0.f;
             for (int k = 0; k < bw; k++) s = fmaf(row[k], V[(b0 + k) * r + q], s);
             V[i * r + q] -= s;
@@ -361,17 +361,20 @@ __global__ void batch_ir_kernel(double *data, const BatchSys *sys, const long lo
         int *piv = reinterpret_cast<int *>(w + ir_align16((size_t)n * n * 4));
         double *X = reinterpret_cast<double *>(w + ir_align16((size_t)n * n * 4) + ir_align16((size_t)n * 4));
         double *R = X + (size_t)n * r;
-        const bool in_smem = (long)n * n + (long)n * r <= smem_floats;
+        // in shared memory with an odd row stride (a column's rows in distinct banks)
+        const int fso = n | 1;
+        const bool in_smem = (long)n * fso + (long)n * r <= smem_floats;
+        const int fs = in_smem ? fso : n;
         float *F = in_smem ? ism : Fg;
-        float *V = in_smem ? ism + (size_t)n * n : ism + (size_t)n * (pw + 1) + (size_t)pw * 64;
+        float *V = in_smem ? ism + (size_t)n * fs : ism + (size_t)n * (pw + 1) + (size_t)pw * 64;
         if (tid == 0) s_zero = 0;
         for (int idx = tid; idx < n * n; idx += T) {
             const int i = idx / n, j = idx - i * n;
-            F[idx] = (float)A[(size_t)i * S.ld + j];
+            F[(size_t)i * fs + j] = (float)A[(size_t)i * S.ld + j];
         }
         __syncthreads();
         if (in_smem)
-            ir_factor_smem(F, n, piv, &s_zero, s_v, s_i);
+            ir_factor_smem(F, n, fs, piv, &s_zero, s_v, s_i);
         else
             ir_factor_blocked(F, n, pw, ism, ism + (size_t)n * (pw + 1), piv, s_dinv, &s_zero, s_v, s_i);
         __syncthreads();
@@ -388,7 +391,7 @@ __global__ void batch_ir_kernel(double *data, const BatchSys *sys, const long lo
             for (it = 1; it <= max_iter; it++) {
                 for (int idx = tid; idx < n * r; idx += T) V[idx] = (float)R[idx];
                 __syncthreads();
-                ir_solve(F, n, piv, V, r);
+                ir_solve(F, n, fs, piv, V, r);
                 for (int idx = tid; idx < n * r; idx += T) X[idx] += (double)V[idx];
                 __syncthreads();
                 ir_residual(A, S.ld, n, r, X, R, false, s_red, s_rmax, s_xmax, s_bmax, &s_anorm);
