@@ -330,6 +330,24 @@ const char *lu2gpu_timer_name(int phase);
 /* Number of CUDA kernels this library has launched in the process so far. */
 long lu2gpu_kernel_launches(void);
 
+/* Fault-path test hook (no counterpart in the reference): the panel leaf of
+ * ctx's later factorizations gives up its cross-CTA waits after wait_ms
+ * milliseconds (0 restores the default, 2000), and, when cta >= 0, CTA `cta`
+ * of every leaf skips its publications, so that every wait of that leaf runs
+ * out.  The call then returns LU2GPU_ERR_TIMEOUT; kernels after the failed
+ * one do nothing that depends on the pivots it never wrote, and the context
+ * stays usable.  lu2gpu_test_leaf_withhold(ctx, -1, 0) switches it off. */
+int lu2gpu_test_leaf_withhold(lu2gpu_ctx *ctx, int cta, double wait_ms);
+
+/* lu2.c:251-291 (swaprows_simple_with_scale, as lu2.c:541-554 applies a
+ * panel's pivots) on the device: for k = k0..k1-1 in order, exchange rows k and
+ * ipiv[k] of columns cs..ce-1 of the n-row row-major device matrix a (leading
+ * dimension lda), then multiply row k by dinv[k] (dinv NULL: no scaling).
+ * k1 - k0 <= 512; every ipiv[k] must lie in [k, n), else LU2GPU_ERR_ARG and
+ * a is left unchanged.  Synchronous. */
+int lu2gpu_swaprows_dev(lu2gpu_ctx *ctx, int n, double *a, long lda, int k0, int k1, const int *ipiv,
+                        const double *dinv, int cs, int ce);
+
 /* lu2gpu_lusolve without any device allocation.  No counterpart in the
  * reference: it exists for callers that cannot allocate device memory at the
  * time they solve -- because another allocator already owns the device memory

@@ -48,6 +48,8 @@ struct LeafParams {
     LeafSlot *slots;  // [2][gridDim.x]
     unsigned long long seq0;
     int *status;
+    unsigned long long wait_ns;  // every wait gives up after this long
+    int withhold;                // test hook: this CTA never publishes (-1: none)
 };
 
 // The 32-bit stamp of publication `seq` (never 0, the value of unwritten slots)
@@ -153,7 +155,7 @@ __global__ void __launch_bounds__(LEAF_THREADS) leaf_kernel(LeafParams<T> P)
             s_wi[warp] = bi;
         }
         __syncthreads();  // S1
-        if (warp == 0) {
+        if (warp == 0 && bid != P.withhold) {
             double v = lane < LEAF_WARPS ? s_wv[lane] : -1.0;
             int i = lane < LEAF_WARPS ? s_wi[lane] : INT_MAX;
             warp_argmax(v, i);
@@ -211,7 +213,7 @@ __global__ void __launch_bounds__(LEAF_THREADS) leaf_kernel(LeafParams<T> P)
                         }
                     }
                 if (pending && (++spins & 63u) == 0 &&
-                    (*(volatile int *)&P.status[1] != 0 || globaltimer_ns() - t0 > WAIT_LIMIT_NS)) {
+                    (*(volatile int *)&P.status[1] != 0 || globaltimer_ns() - t0 > P.wait_ns)) {
                     failed = true;
                     break;
                 }
@@ -232,7 +234,7 @@ __global__ void __launch_bounds__(LEAF_THREADS) leaf_kernel(LeafParams<T> P)
                     ok = stamped(hi, tag) && stamped(lo, tag);
                     if (__all_sync(0xffffffffu, ok)) break;
                     const bool late = (tries & 63u) == 0 && (*(volatile int *)&P.status[1] != 0 ||
-                                                             globaltimer_ns() - t0 > WAIT_LIMIT_NS);
+                                                             globaltimer_ns() - t0 > P.wait_ns);
                     if (__any_sync(0xffffffffu, late)) {
                         failed = true;
                         break;
@@ -339,7 +341,8 @@ static cudaError_t launch_leaf_t(T *a, long ld, int n, int c0, int w, int mode, 
     G = (rows + rpc - 1) / rpc;
     const size_t smem = (size_t)rpc * LEAF_LDS * sizeof(T);
     if (smem > (size_t)LEAF_SMEM_MAX) return cudaErrorInvalidConfiguration;
-    LeafParams<T> P{a, ld, n, c0, w, rpc, mode, goff, ipiv, dinv, buf.slots, *buf.seq, status};
+    LeafParams<T> P{a, ld, n, c0, w, rpc, mode, goff, ipiv, dinv, buf.slots, *buf.seq, status, buf.wait_ns,
+                    buf.withhold};
     *buf.seq += (unsigned long long)w;
     void *args[] = {&P};
     count_launch();

@@ -19,143 +19,248 @@ namespace lu2gpu {
 // 1/pivot right after its exchange; row k is final once exchanged, since
 // later pivots only exchange rows > k).
 //
-// Instead of replaying the npiv exchanges element by element (npiv dependent
-// memory round trips), every CTA first builds the composite permutation of the
-// touched rows in shared memory: slots 0..npiv-1 are the rows k0..k1-1, further
-// slots the distinct rows ipiv[k] >= k1 in order of first appearance; the
-// exchanges are replayed on slot indices only.  Then the CTA gathers the
-// source rows of its 16 columns (128-byte row segments) into shared memory and
-// scatters them to their destinations.
-constexpr int SWAP_COLS = 16;
+// The npiv exchanges (row k <-> row p_k, k = k0..k1-1 in order, p_k >= k)
+// compose to one permutation of at most 2 npiv rows, which every CTA derives
+// in parallel in shared memory:
+//   A(k)  = the original row sitting at position k just before step k: the
+//           row A(i) moved there by the latest step i < k with p_i = k, else k
+//           itself -- a chain i -> k resolved by pointer jumping
+//           (ceil(log2 npiv) rounds);
+//   row k (k0 <= k < k1) finally holds what position p_k held before step k:
+//           A(k) if p_k = k, else A(j) for the latest j < k with p_j = p_k,
+//           else the original row p_k;
+//   row q >= k1 (some p_j = q) finally holds A(j) for the last such j.
+// Then each CTA gathers the source rows of its column chunks (one 128-byte
+// line per row, 16-byte loads, eight in flight per thread) into shared
+// memory and scatters them to their destinations, scaling the pivot rows.
+// Pivots outside [k, nrows) are refused (ERR_BAD_ARG, nothing written), and
+// nothing is done once an earlier wait of the same call has given up (its
+// pivots were never written).
 constexpr int SWAP_THREADS = 256;
+constexpr int SWAP_MAX_PIV = 512;
 
+template <typename T, int V>
+struct SwapVec;
+template <>
+struct SwapVec<double, 2> {
+    using type = double2;
+};
+template <>
+struct SwapVec<float, 4> {
+    using type = float4;
+};
 template <typename T>
-__global__ void __launch_bounds__(SWAP_THREADS) laswp_scale_kernel(T *a, long ld, int k0, int k1,
+struct SwapVec<T, 1> {
+    using type = T;
+};
+
+template <typename T, int V>
+__device__ __forceinline__ void swap_ld(const T *p, int avail, T *out)
+{
+    if (avail >= V) {
+        const typename SwapVec<T, V>::type x = *reinterpret_cast<const typename SwapVec<T, V>::type *>(p);
+        const T *e = reinterpret_cast<const T *>(&x);
+#pragma unroll
+        for (int q = 0; q < V; q++) out[q] = e[q];
+    } else {
+#pragma unroll
+        for (int q = 0; q < V; q++) out[q] = (q < avail) ? p[q] : T(0);
+    }
+}
+
+template <typename T, int V>
+__device__ __forceinline__ void swap_st(T *p, int avail, const T *in)
+{
+    if (avail >= V) {
+        typename SwapVec<T, V>::type x;
+        T *e = reinterpret_cast<T *>(&x);
+#pragma unroll
+        for (int q = 0; q < V; q++) e[q] = in[q];
+        *reinterpret_cast<typename SwapVec<T, V>::type *>(p) = x;
+    } else {
+#pragma unroll
+        for (int q = 0; q < V; q++)
+            if (q < avail) p[q] = in[q];
+    }
+}
+
+template <typename T, int V>
+__global__ void __launch_bounds__(SWAP_THREADS) laswp_scale_kernel(T *a, long ld, int nrows, int k0, int k1,
                                                                    const int *__restrict__ ipiv, int goff,
                                                                    const T *__restrict__ dinv, int cs, int ce,
-                                                                   int scale)
+                                                                   int scale, int *status)
 {
-    extern __shared__ int sw[];
+    constexpr int COLS = 128 / (int)sizeof(T);  // one 128-byte line of a row per chunk
+    constexpr int TPR = COLS / V;               // threads per row segment
+    constexpr int RPP = SWAP_THREADS / TPR;     // rows per pass
+    constexpr int U = 8;                        // loads in flight per thread
+    extern __shared__ __align__(16) unsigned char swap_smem[];
     const int npiv = k1 - k0;
-    int *prow = sw;               // [npiv] view row of each pivot
-    int *first = prow + npiv;     // [npiv] index of the first pivot naming the same row (rows >= k1)
-    int *slot = first + npiv;     // [npiv] extra slot of a first occurrence
-    int *cur = slot + npiv;       // [2 npiv] slot content
-    int *rowof = cur + 2 * npiv;  // [2 npiv] row of each slot
-    __shared__ int s_nslot;
-    T *V = reinterpret_cast<T *>(sw + ((7 * npiv + 1) & ~1));  // [2 npiv][SWAP_COLS], 8-byte aligned
+    T *S = reinterpret_cast<T *>(swap_smem);     // [2 npiv][COLS] staged row segments
+    int *P = reinterpret_cast<int *>(S + (size_t)2 * npiv * COLS);
+    int *A = P + npiv;        // chain pointer (>= 0) or root code -(row)-1
+    int *src = A + npiv;      // [2 npiv] source row of each slot
+    int *dst = src + 2 * npiv; // [2 npiv] destination row of each slot
+    __shared__ int s_nslot, s_bad;
     const int tid = threadIdx.x;
 
-    for (int t = tid; t < npiv; t += SWAP_THREADS) {
-        prow[t] = __ldg(ipiv + k0 + t) - goff;
-        rowof[t] = k0 + t;
-    }
-    for (int s = tid; s < 2 * npiv; s += SWAP_THREADS) cur[s] = s;
-    __syncthreads();
-    for (int t = tid; t < npiv; t += SWAP_THREADS) {
-        const int p = prow[t];
-        int f = -1;
-        if (p >= k1) {
-            f = t;
-            for (int q = 0; q < t; q++)
-                if (prow[q] == p) {
-                    f = q;
-                    break;
-                }
-        }
-        first[t] = f;
-    }
-    __syncthreads();
+    if (status && *(volatile int *)&status[1] != 0) return;
     if (tid == 0) {
-        int nex = 0;
-        for (int t = 0; t < npiv; t++) {
-            const int p = prow[t];
-            int b;
-            if (p < k1) {
-                b = p - k0;
-            } else {
-                const int f = first[t];
-                if (f == t) {
-                    slot[t] = npiv + nex;
-                    rowof[npiv + nex] = p;
-                    nex++;
-                }
-                b = slot[f];
+        s_bad = 0;
+        s_nslot = npiv;
+    }
+    __syncthreads();
+    for (int t = tid; t < npiv; t += SWAP_THREADS) {
+        const int p = __ldg(ipiv + k0 + t) - goff;
+        P[t] = p;
+        A[t] = -1;
+        if (p < k0 + t || p >= nrows) s_bad = 1;
+    }
+    __syncthreads();
+    if (s_bad) {
+        if (blockIdx.x == 0 && tid == 0 && status) record_error(status, ERR_BAD_ARG, 3);
+        return;
+    }
+    for (int i = tid; i < npiv; i += SWAP_THREADS) {
+        const int q = P[i];
+        if (q != k0 + i && q < k1) atomicMax(&A[q - k0], i);
+    }
+    __syncthreads();
+    for (int t = tid; t < npiv; t += SWAP_THREADS)
+        if (A[t] < 0) A[t] = -(k0 + t) - 1;
+    __syncthreads();
+    {
+        // pointer jumping, double-buffered through src (free until the slots
+        // are written): after r rounds every pointer has advanced 2^r links or
+        // reached its root, and a chain has fewer than npiv links
+        int *cur = A, *nxt = src;
+        for (int span = 1; span < npiv; span <<= 1) {
+            for (int t = tid; t < npiv; t += SWAP_THREADS) {
+                const int v = cur[t];
+                nxt[t] = (v >= 0) ? cur[v] : v;
             }
-            const int tmp = cur[t];
-            cur[t] = cur[b];
-            cur[b] = tmp;
+            __syncthreads();
+            int *tmp = cur;
+            cur = nxt;
+            nxt = tmp;
         }
-        s_nslot = npiv + nex;
+        if (cur != A) {
+            for (int t = tid; t < npiv; t += SWAP_THREADS) A[t] = cur[t];
+            __syncthreads();
+        }
+    }
+    for (int t = tid; t < npiv; t += SWAP_THREADS) {
+        const int p = P[t], k = k0 + t;
+        int s;
+        if (p == k) {
+            s = -A[t] - 1;
+        } else {
+            int j = t - 1;
+            while (j >= 0 && P[j] != p) j--;
+            s = (j >= 0) ? -A[j] - 1 : p;
+            if (p >= k1) {
+                int q = t + 1;
+                while (q < npiv && P[q] != p) q++;
+                if (q == npiv) {  // the last exchange that names row p
+                    const int e = atomicAdd(&s_nslot, 1);
+                    src[e] = -A[t] - 1;
+                    dst[e] = p;
+                }
+            }
+        }
+        src[t] = s;
+        dst[t] = k;
     }
     __syncthreads();
     const int nslot = s_nslot;
-    const int c = tid & (SWAP_COLS - 1);
-    const int nchunk = (ce - cs + SWAP_COLS - 1) / SWAP_COLS;
+    const int cq = (tid % TPR) * V, r0 = tid / TPR;
+    const int nchunk = (ce - cs + COLS - 1) / COLS;
     for (int chunk = blockIdx.x; chunk < nchunk; chunk += gridDim.x) {
-        const int j = cs + chunk * SWAP_COLS + c;
-        const bool jok = j < ce;
-        // gather with GATHER_U loads in flight per thread
-        constexpr int STEP = SWAP_THREADS / SWAP_COLS, GATHER_U = 8;
-        for (int s0 = tid / SWAP_COLS; s0 < nslot; s0 += GATHER_U * STEP) {
-            T v[GATHER_U];
+        const int j = cs + chunk * COLS + cq;
+        const int avail = ce - j;
+        for (int s0 = r0; s0 < nslot; s0 += U * RPP) {
+            T v[U][V];
 #pragma unroll
-            for (int u = 0; u < GATHER_U; u++) {
-                const int s = s0 + u * STEP;
-                v[u] = (jok && s < nslot) ? a[(size_t)rowof[cur[s]] * ld + j] : T(0);
+            for (int u = 0; u < U; u++) {
+                const int s = s0 + u * RPP;
+                if (s < nslot && avail > 0) {
+                    swap_ld<T, V>(a + (size_t)src[s] * ld + j, avail, v[u]);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < V; q++) v[u][q] = T(0);
+                }
             }
 #pragma unroll
-            for (int u = 0; u < GATHER_U; u++) {
-                const int s = s0 + u * STEP;
-                if (s < nslot) V[s * SWAP_COLS + c] = v[u];
+            for (int u = 0; u < U; u++) {
+                const int s = s0 + u * RPP;
+                if (s < nslot) swap_st<T, V>(S + (size_t)s * COLS + cq, V, v[u]);
             }
         }
         __syncthreads();
-        if (jok) {
-            for (int s = tid / SWAP_COLS; s < nslot; s += SWAP_THREADS / SWAP_COLS) {
-                T v = V[s * SWAP_COLS + c];
-                if (scale && s < npiv) v *= __ldg(dinv + k0 + s);
-                a[(size_t)rowof[s] * ld + j] = v;
+        if (avail > 0) {
+            for (int s = r0; s < nslot; s += RPP) {
+                T v[V];
+                swap_ld<T, V>(S + (size_t)s * COLS + cq, V, v);
+                if (scale && s < npiv) {
+                    const T d = __ldg(dinv + k0 + s);
+#pragma unroll
+                    for (int q = 0; q < V; q++) v[q] *= d;
+                }
+                swap_st<T, V>(a + (size_t)dst[s] * ld + j, avail, v);
             }
         }
         __syncthreads();
     }
 }
 
-template <typename T>
-static cudaError_t launch_laswp_scale_t(T *a, long ld, int k0, int k1, const int *ipiv, int goff, const T *dinv,
-                                        int cs, int ce, bool scale, cudaStream_t st)
+template <typename T, int V>
+static cudaError_t launch_laswp_v(T *a, long ld, int nrows, int k0, int k1, const int *ipiv, int goff, const T *dinv,
+                                  int cs, int ce, bool scale, int *status, cudaStream_t st)
 {
-    if (ce <= cs || k1 <= k0) return cudaSuccess;
+    constexpr int COLS = 128 / (int)sizeof(T);
     const int npiv = k1 - k0;
-    const size_t smem = (size_t)7 * npiv * sizeof(int) + 8 + (size_t)2 * npiv * SWAP_COLS * sizeof(T);
-    if (smem > 200 * 1024) return cudaErrorInvalidValue;
+    const size_t smem = (size_t)2 * npiv * COLS * sizeof(T) + (size_t)6 * npiv * sizeof(int);
     if (smem > 48 * 1024) {
-        cudaError_t e =
-            cudaFuncSetAttribute(laswp_scale_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        cudaError_t e = cudaFuncSetAttribute(laswp_scale_kernel<T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             200 * 1024);
         if (e != cudaSuccess) return e;
     }
-    // the permutation is built once per CTA; CTAs then stride over 16-column chunks
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    int blocks = (ce - cs + SWAP_COLS - 1) / SWAP_COLS;
-    if (blocks > 3 * sms) blocks = 3 * sms;
+    int per_sm = (int)((220 * 1024) / (smem + 1024));
+    per_sm = per_sm < 1 ? 1 : (per_sm > 4 ? 4 : per_sm);
+    int blocks = (ce - cs + COLS - 1) / COLS;
+    if (blocks > per_sm * sms) blocks = per_sm * sms;
     count_launch();
-    laswp_scale_kernel<T><<<blocks, SWAP_THREADS, smem, st>>>(a, ld, k0, k1, ipiv, goff, dinv, cs, ce, scale ? 1 : 0);
+    laswp_scale_kernel<T, V><<<blocks, SWAP_THREADS, smem, st>>>(a, ld, nrows, k0, k1, ipiv, goff, dinv, cs, ce,
+                                                                  scale ? 1 : 0, status);
     return cudaGetLastError();
 }
 
-cudaError_t launch_laswp_scale(double *a, long ld, int k0, int k1, const int *ipiv, int goff, const double *dinv,
-                               int cs, int ce, bool scale, cudaStream_t st)
+template <typename T>
+static cudaError_t launch_laswp_scale_t(T *a, long ld, int nrows, int k0, int k1, const int *ipiv, int goff,
+                                        const T *dinv, int cs, int ce, bool scale, int *status, cudaStream_t st)
 {
-    return launch_laswp_scale_t(a, ld, k0, k1, ipiv, goff, dinv, cs, ce, scale, st);
+    if (ce <= cs || k1 <= k0) return cudaSuccess;
+    if (k1 - k0 > SWAP_MAX_PIV || k0 < 0 || k1 > nrows) return cudaErrorInvalidValue;
+    constexpr int VW = 16 / (int)sizeof(T);
+    // 16-byte accesses when every row segment starts on a 16-byte boundary
+    if ((reinterpret_cast<uintptr_t>(a) & 15) == 0 && ld % VW == 0 && cs % VW == 0)
+        return launch_laswp_v<T, VW>(a, ld, nrows, k0, k1, ipiv, goff, dinv, cs, ce, scale, status, st);
+    return launch_laswp_v<T, 1>(a, ld, nrows, k0, k1, ipiv, goff, dinv, cs, ce, scale, status, st);
 }
 
-cudaError_t launch_laswp_scale(float *a, long ld, int k0, int k1, const int *ipiv, int goff, const float *dinv,
-                               int cs, int ce, bool scale, cudaStream_t st)
+cudaError_t launch_laswp_scale(double *a, long ld, int nrows, int k0, int k1, const int *ipiv, int goff,
+                               const double *dinv, int cs, int ce, bool scale, int *status, cudaStream_t st)
 {
-    return launch_laswp_scale_t(a, ld, k0, k1, ipiv, goff, dinv, cs, ce, scale, st);
+    return launch_laswp_scale_t(a, ld, nrows, k0, k1, ipiv, goff, dinv, cs, ce, scale, status, st);
+}
+
+cudaError_t launch_laswp_scale(float *a, long ld, int nrows, int k0, int k1, const int *ipiv, int goff,
+                               const float *dinv, int cs, int ce, bool scale, int *status, cudaStream_t st)
+{
+    return launch_laswp_scale_t(a, ld, nrows, k0, k1, ipiv, goff, dinv, cs, ce, scale, status, st);
 }
 
 // ---------------------------------------------------------------------------

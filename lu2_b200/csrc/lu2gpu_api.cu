@@ -258,6 +258,17 @@ extern "C" int lu2gpu_set_stream(lu2gpu_ctx *c, void *stream)
 
 extern "C" const char *lu2gpu_last_error(void) { return g_err; }
 
+extern "C" int lu2gpu_test_leaf_withhold(lu2gpu_ctx *c, int cta, double wait_ms)
+{
+    if (!c || !(wait_ms >= 0.0) || wait_ms > 2000.0) {
+        set_error("lu2gpu_test_leaf_withhold: bad arguments");
+        return LU2GPU_ERR_ARG;
+    }
+    c->leaf.withhold = cta >= 0 ? cta : -1;
+    c->leaf.wait_ns = wait_ms > 0.0 ? (unsigned long long)(wait_ms * 1e6) : WAIT_LIMIT_NS;
+    return 0;
+}
+
 extern "C" int lu2gpu_set_abort_on_error(int on)
 {
     int old = g_abort_on_error;
@@ -348,6 +359,10 @@ static int end_status(lu2gpu_ctx *c, const char *what)
     int st[4];
     CU_TRY(cudaMemcpy(st, c->d_status, sizeof(st), cudaMemcpyDeviceToHost));
     if (st[1] != 0) {
+        if (st[1] == ERR_BAD_ARG) {
+            set_error("%s: a pivot index outside [k, n) was refused on the device (kernel %d)", what, st[2]);
+            return LU2GPU_ERR_ARG;
+        }
         set_error("%s: a bounded device wait gave up (error bits 0x%x, kernel %d)", what, st[1], st[2]);
         return LU2GPU_ERR_TIMEOUT;
     }
@@ -387,9 +402,17 @@ static int right_part(lu2gpu_ctx *c, const View &v, int k0, int k1, int cs, int 
     const int K = k1 - k0;
     {
         PhaseTimer t(c, top ? PH_SWAP : PH_PANEL);
-        K_TRY(launch_laswp_scale(v.a, v.ld, k0, k1, ipiv, v.goff, dinv, cs, ce, true, c->stream));
+        K_TRY(launch_laswp_scale(v.a, v.ld, v.n, k0, k1, ipiv, v.goff, dinv, cs, ce, true, c->d_status, c->stream));
     }
-    double *bt = (!top && c->d_btp) ? c->d_btp : c->d_bt;
+    // inner right parts of a panel (K x (ce - cs) <= nb^2 / 4) use their own
+    // buffer, so that a panel factored beside a running update (which reads
+    // d_bt) never writes d_bt; wider blocks go to d_bt
+    const size_t bt_bytes = (size_t)(ce - cs) * K * sizeof(double);
+    double *bt = (!top && c->d_btp && bt_bytes <= c->btp_cap) ? c->d_btp : c->d_bt;
+    if (bt == c->d_bt && bt_bytes > c->bt_cap) {
+        set_error("right part: transposed U block of %zu bytes exceeds its %zu-byte buffer", bt_bytes, c->bt_cap);
+        return LU2GPU_ERR_ARG;
+    }
     {
         PhaseTimer t(c, top ? PH_TRSM : PH_PANEL);
         K_TRY(launch_trsm_unit_lower(v.a, v.ld, k0, K, cs, ce, bt, c->stream));
@@ -410,8 +433,8 @@ static int right_part_split(lu2gpu_ctx *c, const View &v, int k0, int k1, int cs
 {
     if (ce <= cs) return hook();
     const int K = k1 - k0;
-    K_TRY(launch_laswp_scale(v.a, v.ld, k0, k1, c->d_ipiv + v.goff, v.goff, c->d_dinv + v.goff, cs, ce, true,
-                             c->stream));
+    K_TRY(launch_laswp_scale(v.a, v.ld, v.n, k0, k1, c->d_ipiv + v.goff, v.goff, c->d_dinv + v.goff, cs, ce, true,
+                             c->d_status, c->stream));
     K_TRY(launch_trsm_unit_lower(v.a, v.ld, k0, K, cs, ce, c->d_bt, c->stream));
     if (k1 >= v.n) return hook();
     if (w1 > ce - cs) w1 = ce - cs;
@@ -444,19 +467,24 @@ static int panel(lu2gpu_ctx *c, const View &v, int c0, int m, int mode)
     rc = panel(c, v, c0 + h, m - h, mode);
     if (rc) return rc;
     PhaseTimer t(c, PH_PANEL);
-    K_TRY(launch_laswp_scale(v.a, v.ld, c0 + h, c0 + m, c->d_ipiv + v.goff, v.goff, c->d_dinv + v.goff, c0, c0 + h,
-                             true, c->stream));
+    K_TRY(launch_laswp_scale(v.a, v.ld, v.n, c0 + h, c0 + m, c->d_ipiv + v.goff, v.goff, c->d_dinv + v.goff, c0,
+                             c0 + h, true, c->d_status, c->stream));
     return 0;
 }
 
 static int ensure_work(lu2gpu_ctx *c, int n, int ncols, int nb)
 {
     size_t need_bt = (size_t)ncols * (size_t)nb + 1024;
+    if (c->fixed_scratch) {  // lu2gpu_lusolve_noalloc: its buffers are fixed, never grown
+        if (need_bt * sizeof(double) > c->bt_cap || (size_t)n > c->piv_cap) {
+            set_error("fixed scratch too small for n=%d, %d columns, nb=%d", n, ncols, nb);
+            return LU2GPU_ERR_ARG;
+        }
+        return 0;
+    }
     int rc = grow((void **)&c->d_bt, &c->bt_cap, need_bt * sizeof(double));
     if (rc) return rc;
-    if (!c->fixed_scratch &&
-        (rc = grow((void **)&c->d_btp, &c->btp_cap, ((size_t)nb * nb + 1024) * sizeof(double))))
-        return rc;
+    if ((rc = grow((void **)&c->d_btp, &c->btp_cap, ((size_t)nb * nb + 1024) * sizeof(double)))) return rc;
     if (c->piv_cap < (size_t)n) {
         cudaFree(c->d_ipiv);
         cudaFree(c->d_dinv);
@@ -738,7 +766,7 @@ extern "C" int lu2gpu_solve(lu2gpu_ctx *c, int n, const double *a, long lda, int
     K_TRY(launch_diag_inv(a, lda, n, c->d_dinv, c->stream));
     for (int i = 0; i < n; i += nb) {
         const int w = (n - i) < nb ? (n - i) : nb;
-        K_TRY(launch_laswp_scale(b, ldb, i, i + w, ipiv, 0, c->d_dinv, 0, nrhs, true, c->stream));
+        K_TRY(launch_laswp_scale(b, ldb, n, i, i + w, ipiv, 0, c->d_dinv, 0, nrhs, true, c->d_status, c->stream));
         K_TRY(launch_trsm_unit_lower_tx(a + (size_t)i * lda + i, lda, b + (size_t)i * ldb, ldb, w, nrhs, c->d_bt,
                                         c->stream));
         if (i + w < n)
@@ -793,6 +821,23 @@ extern "C" int lu2gpu_dgemm_dev(lu2gpu_ctx *c, int m, int n, int k, double alpha
     }
     K_TRY(launch_dgemm_general(x, ldx, y, ldy, cm, ldc, m, n, kk, alpha, beta, c->d_status, c->stream));
     return end_status(c, "lu2gpu_dgemm_dev");
+}
+
+// lu2.c:251-291 over a panel's pivots, as lu2.c:541-554 applies them
+extern "C" int lu2gpu_swaprows_dev(lu2gpu_ctx *c, int n, double *a, long lda, int k0, int k1, const int *ipiv,
+                                   const double *dinv, int cs, int ce)
+{
+    if (!c || n <= 0 || !a || !ipiv || k0 < 0 || k1 < k0 || k1 > n || k1 - k0 > 512 || cs < 0 || ce < cs ||
+        lda < ce) {
+        set_error("lu2gpu_swaprows_dev: bad arguments");
+        return LU2GPU_ERR_ARG;
+    }
+    if (k1 == k0 || ce == cs) return 0;
+    DeviceGuard g(c->device);
+    int rc = begin_status(c);
+    if (rc) return rc;
+    K_TRY(launch_laswp_scale(a, lda, n, k0, k1, ipiv, 0, dinv, cs, ce, dinv != nullptr, c->d_status, c->stream));
+    return end_status(c, "lu2gpu_swaprows_dev");
 }
 
 // ---------------------------------------------------------------------------
@@ -1316,8 +1361,8 @@ static int right_part_anyk(lu2gpu_ctx *c, const View &v, int k0, int k1, int cs,
     if (ce <= cs) return 0;
     if ((k1 - k0) % 16 == 0) return right_part(c, v, k0, k1, cs, ce, false);
     const int K = k1 - k0;
-    K_TRY(launch_laswp_scale(v.a, v.ld, k0, k1, c->d_ipiv + v.goff, v.goff, c->d_dinv + v.goff, cs, ce, true,
-                             c->stream));
+    K_TRY(launch_laswp_scale(v.a, v.ld, v.n, k0, k1, c->d_ipiv + v.goff, v.goff, c->d_dinv + v.goff, cs, ce, true,
+                             c->d_status, c->stream));
     K_TRY(launch_trsm_unit_lower(v.a, v.ld, k0, K, cs, ce, c->d_bt, c->stream));
     if (k1 < v.n) {
         const long ldk = (K + 1) & ~1L;
@@ -1608,6 +1653,7 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH
 static std::mutex g_noalloc_mu;
 static void *g_noalloc_ptr[128];
 static int g_noalloc_ctas[128];
+static int g_noalloc_major[128];  // compute capability major of each device, 0 until looked up
 // leaf publication stamps per device; the slots start zeroed (static storage)
 // and every stamp is used once, so leftovers of earlier calls never match
 static unsigned long long g_noalloc_seq[128];
@@ -1619,6 +1665,20 @@ static int noalloc_setup(int device, unsigned char **base, int *leaf_ctas)
         return LU2GPU_ERR_ARG;
     }
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_major[device]) {
+        int major = 0;
+        if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device) != cudaSuccess) {
+            cudaGetLastError();
+            set_error("lu2gpu_lusolve_noalloc: no usable CUDA device %d", device);
+            return LU2GPU_ERR_NODEV;
+        }
+        g_noalloc_major[device] = major;
+    }
+    if (g_noalloc_major[device] != 10) {
+        set_error("lu2gpu_lusolve_noalloc: device %d is sm_%d*; this library is built for sm_100a only", device,
+                  g_noalloc_major[device]);
+        return LU2GPU_ERR_NODEV;
+    }
     if (!g_noalloc_ptr[device]) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
@@ -1802,7 +1862,7 @@ static int right_part32(lu2gpu_ctx *c, const View32 &v, int k0, int k1, int cs, 
     const int K = k1 - k0;
     {
         PhaseTimer t(c, top ? PH_SWAP : PH_PANEL);
-        K_TRY(launch_laswp_scale(v.a, v.ld, k0, k1, ipiv, v.goff, dinv, cs, ce, true, c->stream));
+        K_TRY(launch_laswp_scale(v.a, v.ld, v.n, k0, k1, ipiv, v.goff, dinv, cs, ce, true, c->d_status, c->stream));
     }
     const float *T = v.a + (size_t)k0 * v.ld + k0;
     float *X = v.a + (size_t)k0 * v.ld + cs;
@@ -1829,7 +1889,7 @@ static int right_part32_split(lu2gpu_ctx *c, const View32 &v, int k0, int k1, in
     if (w1 <= 0 || w1 >= N || (w1 % 128)) w1 = N;
     {
         PhaseTimer t(c, PH_SWAP);
-        K_TRY(launch_laswp_scale(v.a, v.ld, k0, k1, ipiv, v.goff, dinv, cs, ce, true, c->stream));
+        K_TRY(launch_laswp_scale(v.a, v.ld, v.n, k0, k1, ipiv, v.goff, dinv, cs, ce, true, c->d_status, c->stream));
     }
     const float *T = v.a + (size_t)k0 * v.ld + k0;
     float *X = v.a + (size_t)k0 * v.ld + cs;
@@ -1903,8 +1963,8 @@ static int panel32(lu2gpu_ctx *c, const View32 &v, int c0, int m, int mode)
     if ((rc = right_part32(c, v, c0, c0 + h, c0 + h, c0 + m, false))) return rc;
     if ((rc = panel32(c, v, c0 + h, m - h, mode))) return rc;
     PhaseTimer t(c, PH_PANEL);
-    K_TRY(launch_laswp_scale(v.a, v.ld, c0 + h, c0 + m, c->d_ipiv + v.goff, v.goff, c->mx->dinv + v.goff, c0, c0 + h,
-                             true, c->stream));
+    K_TRY(launch_laswp_scale(v.a, v.ld, v.n, c0 + h, c0 + m, c->d_ipiv + v.goff, v.goff, c->mx->dinv + v.goff, c0,
+                             c0 + h, true, c->d_status, c->stream));
     return 0;
 }
 
@@ -1915,7 +1975,7 @@ static int solve32_enqueue(lu2gpu_ctx *c, int n, const float *a, long ld, int nb
     MixedWork *m = c->mx;
     for (int i = 0; i < n; i += nb) {
         const int w = (n - i) < nb ? (n - i) : nb;
-        K_TRY(launch_laswp_scale(v, 1, i, i + w, c->d_ipiv, 0, m->dinv, 0, 1, true, c->stream));
+        K_TRY(launch_laswp_scale(v, 1, n, i, i + w, c->d_ipiv, 0, m->dinv, 0, 1, true, c->d_status, c->stream));
         K_TRY(launch_trsm_unit_lower_f32(a + (size_t)i * ld + i, ld, v + i, 1, w, 1, nullptr, c->stream));
         if (i + w < n)
             K_TRY(launch_gemv_sub(a + (size_t)(i + w) * ld + i, ld, n - i - w, w, v + i, v + i + w, c->stream));

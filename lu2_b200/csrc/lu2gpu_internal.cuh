@@ -81,8 +81,13 @@ struct __align__(64) LeafSlot {
 };
 
 struct LeafBuffers {
-    LeafSlot *slots;          // [2][max CTAs], zeroed once
-    unsigned long long *seq;  // host-side stamp counter, advanced by every leaf launch
+    LeafSlot *slots = nullptr;          // [2][max CTAs], zeroed once
+    unsigned long long *seq = nullptr;  // host-side stamp counter, advanced by every leaf launch
+    // fault-path test hook (lu2gpu_test_leaf_withhold): the wait limit of the
+    // exchange, and a CTA that skips its publications (-1: none) so that every
+    // other CTA's wait runs out
+    unsigned long long wait_ns = WAIT_LIMIT_NS;
+    int withhold = -1;
 };
 
 // Factor the leaf panel: rows c0..n-1, columns c0..c0+w-1 (w <= 16) of the
@@ -96,13 +101,15 @@ int leaf_max_ctas(int device);
 // fewest leaf CTAs whose slabs of `rows` rows (elements of tsize bytes) fit shared memory
 int leaf_min_ctas(int rows, size_t tsize);
 
-// Apply the pivots k0..k1-1 (row k <-> row ipiv[k], in order) to columns
-// cs..ce-1 and, when `scale`, multiply row k by dinv[k] after its swap.
-// ipiv holds global rows; the view's row is ipiv[k] - goff.
-cudaError_t launch_laswp_scale(double *a, long ld, int k0, int k1, const int *ipiv, int goff, const double *dinv,
-                               int cs, int ce, bool scale, cudaStream_t st);
-cudaError_t launch_laswp_scale(float *a, long ld, int k0, int k1, const int *ipiv, int goff, const float *dinv,
-                               int cs, int ce, bool scale, cudaStream_t st);
+// Apply the pivots k0..k1-1 (row k <-> row ipiv[k], in order; k1 - k0 <= 512)
+// to columns cs..ce-1 of the nrows-row matrix and, when `scale`, multiply row
+// k by dinv[k] after its swap.  ipiv holds global rows; the view's row is
+// ipiv[k] - goff.  A pivot outside [k, nrows) sets ERR_BAD_ARG in status[1]
+// and nothing is written; with status[1] already nonzero nothing is done.
+cudaError_t launch_laswp_scale(double *a, long ld, int nrows, int k0, int k1, const int *ipiv, int goff,
+                               const double *dinv, int cs, int ce, bool scale, int *status, cudaStream_t st);
+cudaError_t launch_laswp_scale(float *a, long ld, int nrows, int k0, int k1, const int *ipiv, int goff,
+                               const float *dinv, int cs, int ce, bool scale, int *status, cudaStream_t st);
 
 // In place X := T^{-1} X for the unit lower triangle T = strict lower part of
 // a[r0..r0+K)[r0..r0+K) and X = a[r0..r0+K)[cs..ce); also writes

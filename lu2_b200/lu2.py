@@ -205,6 +205,16 @@ class Context:
         _check("lu2gpu_dgemm_dev",
                lib().lu2gpu_dgemm_dev(self._h, m, n, k, alpha, _ptr(a), lda, _ptr(b), ldb, beta, _ptr(c), ldc))
 
+    def swaprows(self, a, n: int, lda: int, k0: int, k1: int, ipiv, dinv, cs: int, ce: int) -> None:
+        """lu2's row exchanges of a panel (rows k <-> ipiv[k], k = k0..k1-1, then
+        row k *= dinv[k]) on columns cs..ce-1 of the device matrix a."""
+        _check("lu2gpu_swaprows_dev", lib().lu2gpu_swaprows_dev(self._h, n, _ptr(a), lda, k0, k1, _ptr(ipiv),
+                                                                 _ptr(dinv) if dinv is not None else None, cs, ce))
+
+    def test_leaf_withhold(self, cta: int, wait_ms: float) -> None:
+        """Fault-path test hook: leaf waits give up after wait_ms; CTA `cta` skips its publications."""
+        _check("lu2gpu_test_leaf_withhold", lib().lu2gpu_test_leaf_withhold(self._h, cta, wait_ms))
+
     def pivots(self, n: int) -> np.ndarray:
         out = np.zeros(n, dtype=np.int32)
         _check("lu2gpu_copy_pivots", lib().lu2gpu_copy_pivots(self._h, _ptr(out), n))

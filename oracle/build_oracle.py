@@ -29,7 +29,10 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_DIR = os.environ.get("LU2_REFERENCE_DIR", "/root/reference")
+# the telmin/lu2 checkout: LU2_REFERENCE_DIR, else a directory "reference"
+# beside this repository
+REF_DIR = os.environ.get("LU2_REFERENCE_DIR",
+                         os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
 OUT_DIR = os.path.join(HERE, "_ref")
 
 REF_SOURCES = ["lu2lib.c", "timerlib.c", "second.c", "lu2_mp_nompi.c"]

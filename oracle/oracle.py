@@ -82,6 +82,8 @@ class RefLib:
         L.ref_lu2_factor_solve.restype = C.c_int
         L.ref_lu2_lumcolumn.argtypes = [C.c_int, C.c_int, C.c_int, _dp, C.POINTER(C.c_double)]
         L.ref_lu2_lumcolumn.restype = C.c_int
+        L.ref_lu2_factor_solve_diag.argtypes = [C.c_int, C.c_int, C.c_int, _dp, _dp, _ip, C.POINTER(C.c_double)]
+        L.ref_lu2_factor_solve_diag.restype = C.c_int
 
     @staticmethod
     def available(variant: str = "shipped") -> bool:
@@ -95,6 +97,17 @@ class RefLib:
         piv = np.zeros(n, dtype=np.int32)
         t = C.c_double(0)
         rc = self.lib.ref_lu2_factor_solve(n, nb, seed, x, piv, C.byref(t))
+        if rc != 0:
+            raise RuntimeError("reference run failed rc=%d" % rc)
+        return x, piv, t.value
+
+    def factor_solve_diag(self, n: int, nb: int, seed: int, diag: np.ndarray):
+        """factor_solve on randomsetmat's matrix with its diagonal replaced by ``diag``."""
+        x = np.zeros(n, dtype=np.float64)
+        piv = np.zeros(n, dtype=np.int32)
+        t = C.c_double(0)
+        rc = self.lib.ref_lu2_factor_solve_diag(n, nb, seed, np.ascontiguousarray(diag, dtype=np.float64), x, piv,
+                                                C.byref(t))
         if rc != 0:
             raise RuntimeError("reference run failed rc=%d" % rc)
         return x, piv, t.value

@@ -1,6 +1,6 @@
 /*
  * ref_harness.c -- drives the UNMODIFIED reference sources (compiled from
- * telmin/lu2 into oracle/_ref/ by oracle/Makefile) so that tests can pin the
+ * telmin/lu2 into oracle/_ref/ by oracle/build_oracle.py) so that tests can pin the
  * oracle restatement against the reference itself, and bench.py can time the
  * reference's own CPU path.
  *
@@ -38,6 +38,7 @@ void omp_set_num_threads(int);
 
 typedef struct {
     int n, nb, seed, which;
+    const double *diag; /* optional: a[i][i] := diag[i] after randomsetmat */
     double *x;
     int *piv;
     double seconds;
@@ -66,6 +67,8 @@ static void *run_job(void *arg)
     }
     memset(a, 0, sizeof(double) * (size_t)n * rdim);
     randomsetmat(n, j->seed, a);
+    if (j->diag)
+        for (int i = 0; i < n; i++) a[(size_t)i * rdim + i] = j->diag[i];
     double t0 = now_s();
     if (j->which == 0) {
         for (int i = 0; i < n; i += nb) {
@@ -112,7 +115,7 @@ void ref_set_threads(int blas_threads, int omp_threads)
 int ref_lu2_factor_solve(int n, int nb, int seed, double *x_out, int *piv_out, double *seconds)
 {
     if (n <= 0 || nb <= 0 || n % nb) return -1;
-    job_t j = {n, nb, seed, 0, x_out, piv_out, 0.0, -1};
+    job_t j = {n, nb, seed, 0, NULL, x_out, piv_out, 0.0, -1};
     int rc = run_on_big_stack(&j);
     if (seconds) *seconds = j.seconds;
     return rc;
@@ -122,7 +125,19 @@ int ref_lu2_factor_solve(int n, int nb, int seed, double *x_out, int *piv_out, d
 int ref_lu2_lumcolumn(int n, int nb, int seed, double *x_out, double *seconds)
 {
     if (n <= 0 || nb <= 0 || n % nb) return -1;
-    job_t j = {n, nb, seed, 1, x_out, NULL, 0.0, -1};
+    job_t j = {n, nb, seed, 1, NULL, x_out, NULL, 0.0, -1};
+    int rc = run_on_big_stack(&j);
+    if (seconds) *seconds = j.seconds;
+    return rc;
+}
+
+/* As ref_lu2_factor_solve, on randomsetmat's matrix with its diagonal replaced
+ * by diag[0..n) (the diagonally dominant, well-conditioned parity cases). */
+int ref_lu2_factor_solve_diag(int n, int nb, int seed, const double *diag, double *x_out, int *piv_out,
+                              double *seconds)
+{
+    if (n <= 0 || nb <= 0 || n % nb || !diag) return -1;
+    job_t j = {n, nb, seed, 0, diag, x_out, piv_out, 0.0, -1};
     int rc = run_on_big_stack(&j);
     if (seconds) *seconds = j.seconds;
     return rc;

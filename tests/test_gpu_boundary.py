@@ -17,10 +17,14 @@ def _p(x):
     return ctypes.c_void_p(x.ctypes.data)
 
 
-@pytest.mark.parametrize("n,nb,seed,variant,mode,xtol",
-                         [(512, 128, 12345, "fixed", L.PIVOT_PARTIAL, 2e-11),
-                          (256, 64, 12345, "shipped", L.PIVOT_REF, 1e-6)])
-def test_lu2_panel_loop_through_boundary(oracle, golden, n, nb, seed, variant, mode, xtol):
+@pytest.mark.parametrize("n,nb,seed,variant,mode",
+                         [(512, 128, 12345, "fixed", L.PIVOT_PARTIAL),
+                          (2048, 256, 1, "fixed", L.PIVOT_PARTIAL),
+                          (256, 64, 12345, "shipped", L.PIVOT_REF)])
+def test_lu2_panel_loop_through_boundary(oracle, golden, parity, n, nb, seed, variant, mode):
+    """Bars as in test_gpu_lu.py: max(1e-12, 2 d_ref) against the fixed
+    reference, 4 d_ref against the shipped one (d_ref = that reference's own
+    forward error against the extended-precision solution)."""
     lib = L.load()
     old = lib.lu2gpu_set_pivot_mode(mode)
     try:
@@ -38,7 +42,11 @@ def test_lu2_panel_loop_through_boundary(oracle, golden, n, nb, seed, variant, m
     key = "%s_n%d_nb%d_s%d" % (variant, n, nb, seed)
     np.testing.assert_array_equal(piv, golden[key + "_piv"])
     xr = golden[key + "_x"]
-    assert np.abs(b - xr).max() / np.abs(xr).max() < xtol
+    xhp = golden["hp_n%d_s%d_x" % (n, seed)]
+    d_ref = np.abs(xr - xhp).max() / np.abs(xhp).max()
+    bar = max(1e-12, 2 * d_ref) if mode == L.PIVOT_PARTIAL else 4 * d_ref
+    parity("lu2 panel loop %s n=%d nb=%d seed=%d" % (variant, n, nb, seed), np.abs(b - xr).max() / np.abs(xr).max(),
+           bar, "fwd err ref %.2e" % d_ref)
 
 
 def _slab(oracle, n, i, cols, seed):

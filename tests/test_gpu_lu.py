@@ -2,11 +2,22 @@
 reference's own results (golden vectors, and the compiled reference at
 n = 8192).
 
-Bars: pivots equal index for index; x within XTOL_PARTIAL (relative, max
-norm) of the fixed reference in partial-pivoting mode, and within XTOL_REF of
-the shipped reference in its bug-compatible mode (that algorithm amplifies
-rounding differences by its poor pivots); HPL scaled residual < 16 in
-partial-pivoting mode."""
+Bars.  Pivots: equal index for index.  x, relative in the max norm:
+
+* partial pivoting against the fixed reference: XTOL_PARTIAL = 1e-12, the
+  agreement asked of the path on well-conditioned inputs.  It holds outright
+  on the diagonally dominant systems.  On lu2's uniform random matrices two
+  correct FP64 LUs already differ by more at n = 2048 (cond ~ 4e5; the fixed
+  reference and LAPACK differ by up to 1.3e-12), so there the bar is
+  max(XTOL_PARTIAL, 2 d_ref), d_ref being the reference's own forward error
+  against the extended-precision solution: a solver as accurate as the
+  reference is within 2 d_ref of it (triangle inequality).
+* the bug-compatible mode against the shipped reference: 4 d_ref.  That
+  algorithm's poor pivots make its rounding error large (1e-12 .. 1e-8), and
+  two evaluation orders differ by about that error.
+
+The GPU's own forward error is reported beside each case.  HPL scaled
+residual < 16 in partial-pivoting mode."""
 import numpy as np
 import pytest
 
@@ -15,10 +26,21 @@ from oracle.oracle import RefLib
 
 pytestmark = pytest.mark.gpu
 
-XTOL_PARTIAL = 2e-11
-XTOL_REF = 1e-6
+XTOL_PARTIAL = 1e-12
+REF_FACTOR = 4.0
 GOLDEN_CASES = [(128, 64, 1), (256, 64, 12345), (512, 128, 12345), (1024, 256, 1), (2048, 64, 1),
                 (2048, 128, 12345), (2048, 256, 1)]
+DD_CASES = [(1024, 64, 1), (2048, 256, 12345), (4096, 256, 1)]
+
+
+def rel(x, y):
+    return float(np.abs(x - y).max() / np.abs(y).max())
+
+
+def x_bar(mode, d_ref):
+    """The bar for x against the reference variant matching `mode`, whose
+    forward error is d_ref."""
+    return max(XTOL_PARTIAL, 2.0 * d_ref) if mode == PIVOT_PARTIAL else REF_FACTOR * d_ref
 
 
 def dev_matrix(ctx, n, seed, nrhs=1, kind=0):
@@ -56,8 +78,8 @@ def test_generator_diagonally_dominant(ctx, oracle):
 
 
 @pytest.mark.parametrize("n,nb,seed", GOLDEN_CASES)
-@pytest.mark.parametrize("variant,mode,xtol", [("fixed", PIVOT_PARTIAL, XTOL_PARTIAL), ("shipped", PIVOT_REF, XTOL_REF)])
-def test_lusolve_matches_reference(ctx, golden, oracle, n, nb, seed, variant, mode, xtol):
+@pytest.mark.parametrize("variant,mode", [("fixed", PIVOT_PARTIAL), ("shipped", PIVOT_REF)])
+def test_lusolve_matches_reference(ctx, golden, oracle, parity, n, nb, seed, variant, mode):
     a, ld = dev_matrix(ctx, n, seed)
     info = ctx.lusolve(a, n, ld, nb, 1, mode)
     assert info == 0
@@ -66,12 +88,38 @@ def test_lusolve_matches_reference(ctx, golden, oracle, n, nb, seed, variant, mo
     np.testing.assert_array_equal(piv, golden[key + "_piv"])
     x = a[:, n].cpu().numpy()
     xr = golden[key + "_x"]
-    assert np.abs(x - xr).max() / np.abs(xr).max() < xtol
+    xhp = golden["hp_n%d_s%d_x" % (n, seed)]
+    d_ref = rel(xr, xhp)
+    parity("lusolve %s n=%d nb=%d seed=%d" % (variant, n, nb, seed), rel(x, xr), x_bar(mode, d_ref),
+           "fwd err gpu %.2e ref %.2e" % (rel(x, xhp), d_ref))
     if mode == PIVOT_PARTIAL:
         assert hpl(oracle.randomsetmat(n, seed), x, n) < 16
 
 
-def test_lumcolumn_host_entry(oracle):
+@pytest.mark.parametrize("n,nb,seed", DD_CASES)
+@pytest.mark.parametrize("variant,mode", [("fixed", PIVOT_PARTIAL), ("shipped", PIVOT_REF)])
+def test_lusolve_well_conditioned_matches_reference(ctx, golden, oracle, parity, n, nb, seed, variant, mode):
+    """Diagonally dominant systems (the reference's matrix with a_ii replaced by
+    the row's absolute sum): x within 1e-12 of the fixed reference."""
+    import torch
+
+    a, ld = dev_matrix(ctx, n, seed)
+    diag = torch.tensor(golden["dd_diag_n%d_s%d" % (n, seed)], device="cuda")
+    idx = torch.arange(n, device="cuda")
+    a[idx, idx] = diag
+    assert ctx.lusolve(a, n, ld, nb, 1, mode) == 0
+    key = "%s_dd_n%d_nb%d_s%d" % (variant, n, nb, seed)
+    np.testing.assert_array_equal(ctx.pivots(n), golden[key + "_piv"])
+    x = a[:, n].cpu().numpy()
+    xr = golden[key + "_x"]
+    xhp = golden["dd_hp_n%d_s%d_x" % (n, seed)]
+    d_ref = rel(xr, xhp)
+    bar = XTOL_PARTIAL if mode == PIVOT_PARTIAL else x_bar(mode, d_ref)
+    parity("lusolve diag-dominant %s n=%d nb=%d seed=%d" % (variant, n, nb, seed), rel(x, xr), bar,
+           "fwd err gpu %.2e ref %.2e" % (rel(x, xhp), d_ref))
+
+
+def test_lumcolumn_host_entry(oracle, golden, parity):
     n, nb, seed = 512, 64, 1
     a = oracle.randomsetmat(n, seed)
     b = np.zeros(n)
@@ -79,8 +127,10 @@ def test_lumcolumn_host_entry(oracle):
     assert lumcolumn(a, b, nb, pv, PIVOT_PARTIAL) == 0
     ao = oracle.randomsetmat(n, seed)
     xo, po = oracle.lumcolumn(ao, n, nb, PIVOT_PARTIAL)
-    assert np.abs(b - xo).max() / np.abs(xo).max() < XTOL_PARTIAL
     np.testing.assert_array_equal(pv, po[n - nb:])
+    xr = golden["fixed_n512_nb64_s1_x"]
+    parity("lumcolumn (host) n=512 nb=64 seed=1 vs fixed reference", rel(b, xr),
+           x_bar(PIVOT_PARTIAL, rel(xr, golden["hp_n512_s1_x"])), "vs oracle %.2e" % rel(b, xo))
     # the factors land in the caller's array in lu2's storage (unit U', y in column n)
     iu = np.triu_indices(n, 1)
     assert np.abs(a[:, :n][iu] - ao[:, :n][iu]).max() < 1e-9
@@ -255,13 +305,34 @@ def test_pivot_ties_go_to_lowest_row(ctx, oracle):
     np.testing.assert_array_equal(ctx.pivots(n), po)
 
 
+def hp_solution(a0, n):
+    """The system's solution refined with long-double residuals (the yardstick
+    of forward errors; the fixtures' hp_* vectors are made the same way)."""
+    import scipy.linalg as sl
+
+    A, b = a0[:, :n], a0[:, n]
+    lu = sl.lu_factor(A)
+    x = sl.lu_solve(lu, b).astype(np.longdouble)
+    Al, bl = A.astype(np.longdouble), b.astype(np.longdouble)
+    for _ in range(3):
+        x = x + sl.lu_solve(lu, (bl - Al @ x).astype(np.float64)).astype(np.longdouble)
+    return x.astype(np.float64)
+
+
+@pytest.fixture(scope="module")
+def n8192_case(oracle):
+    a0 = oracle.randomsetmat(8192, 1)
+    return a0, hp_solution(a0, 8192)
+
+
 @pytest.mark.skipif(not RefLib.available("fixed"), reason="compiled reference not present")
 @pytest.mark.parametrize("variant,mode", [("fixed", PIVOT_PARTIAL), ("shipped", PIVOT_REF)])
-def test_n8192_against_compiled_reference(ctx, oracle, variant, mode):
+def test_n8192_against_compiled_reference(ctx, oracle, parity, n8192_case, variant, mode):
     """Cross-check at N=8192 (nb=256): the compiled reference CPU lu2 on identical inputs."""
     import os
 
     n, nb, seed = 8192, 256, 1
+    a0, xhp = n8192_case
     ref = RefLib(variant)
     ref.set_threads(max(1, min(32, os.cpu_count() or 1)), 1)
     xr, pr, _ = ref.factor_solve(n, nb, seed)
@@ -269,12 +340,10 @@ def test_n8192_against_compiled_reference(ctx, oracle, variant, mode):
     assert ctx.lusolve(a, n, ld, nb, 1, mode) == 0
     piv = ctx.pivots(n)
     x = a[:, n].cpu().numpy()
-    rel = np.abs(x - xr).max() / np.abs(xr).max()
     mism = int((piv != pr).sum())
-    print("n=8192 %s: pivot mismatches %d, x rel diff %.3e" % (variant, mism, rel))
-    assert mism == 0
+    assert mism == 0, "%d pivot mismatches" % mism
+    d_ref = rel(xr, xhp)
+    parity("lusolve %s n=8192 nb=256 seed=1 (live reference)" % variant, rel(x, xr), x_bar(mode, d_ref),
+           "fwd err gpu %.2e ref %.2e" % (rel(x, xhp), d_ref))
     if mode == PIVOT_PARTIAL:
-        assert rel < 1e-10
-        assert hpl(oracle.randomsetmat(n, seed), x, n) < 16
-    else:
-        assert rel < 1e-5
+        assert hpl(a0, x, n) < 16

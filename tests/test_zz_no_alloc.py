@@ -17,7 +17,7 @@ import lu2_b200 as L
 
 pytestmark = pytest.mark.gpu
 
-XTOL = 2e-11  # the partial-pivoting x tolerance of tests/test_gpu_lu.py
+XTOL = 1e-12  # the partial-pivoting x bar of tests/test_gpu_lu.py
 
 
 def _matrix(ctx, n, nrhs, seed):
@@ -58,6 +58,30 @@ def test_noalloc_matches_lusolve_on_two_calls():
         x_na = a_na[:, n:n + nrhs].cpu().numpy()
         assert np.abs(x_na - x_ref).max() / np.abs(x_ref).max() < XTOL, call
     assert free_after[1] == free_after[0]
+    ctx.close()
+
+
+def test_noalloc_at_its_limits_without_pivot_output():
+    """n = 2048, nrhs = 16, nb = 128 (every limit at once) with ipiv = NULL, so
+    the pivots also live in the fixed array."""
+    import torch
+
+    lib = L.load()
+    torch.cuda.set_device(0)
+    ctx = L.Context(0)
+    stream = torch.cuda.current_stream()
+    n, nb, nrhs = 2048, 128, 16
+    a_ref, ld = _matrix(ctx, n, nrhs, 7)
+    a_na = a_ref.clone()
+    torch.cuda.synchronize()
+    assert ctx.lusolve(a_ref, n, ld, nb, nrhs, L.PIVOT_PARTIAL) == 0
+    rc = lib.lu2gpu_lusolve_noalloc(n, nrhs, a_na.data_ptr(), ld, nb, L.PIVOT_PARTIAL, None,
+                                    ctypes.c_void_p(stream.cuda_stream))
+    assert rc == 0, L._lib.last_error()
+    torch.cuda.synchronize()
+    x_ref = a_ref[:, n:n + nrhs].cpu().numpy()
+    x_na = a_na[:, n:n + nrhs].cpu().numpy()
+    assert np.abs(x_na - x_ref).max() / np.abs(x_ref).max() < XTOL
     ctx.close()
 
 
