@@ -120,34 +120,83 @@ class Clocks:
                 "reasons": reasons}
 
 
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def ref_run(ref, n, nb, seed, runs, orc=None):
+    """median GFLOP/s of `runs` timed lumcolumn calls (after one untimed) and
+    the HPL scaled residual of the last x"""
+    ref.lumcolumn(n, nb, seed)
+    ts, x = [], None
+    for _ in range(runs):
+        x, t = ref.lumcolumn(n, nb, seed)
+        ts.append(t)
+    out = {"gflops": lu_flops(n) / statistics.median(ts) / 1e9, "seconds_median": statistics.median(ts)}
+    if orc is not None:
+        out["hpl"] = orc.residual(orc.randomsetmat(n, seed), n, x)["hpl"]
+    return out
+
+
+def c1_baseline(cores: int, runs: int = 5) -> dict:
+    """BASELINE config 1, the reference CPU lu2 (nompi) at N = 2048, nb = 64:
+    shipped and pivot-fixed builds, seeds 1 and 12345, OpenBLAS on every core
+    with one OpenMP thread (the fastest split), median of `runs`; plus the
+    default split (OpenMP and OpenBLAS both on every core), timed once."""
+    from oracle.oracle import OracleLib, RefLib
+
+    orc = OracleLib()
+    out = {}
+    for variant in ("shipped", "fixed"):
+        ref = RefLib(variant)
+        ref.set_threads(cores, 1)
+        for seed in (1, 12345):
+            r = ref_run(ref, 2048, 64, seed, runs, orc)
+            out["c1_%s_s%d_gflops" % (variant, seed)] = r["gflops"]
+            out["c1_%s_s%d_hpl" % (variant, seed)] = r["hpl"]
+    ref = RefLib("shipped")
+    ref.set_threads(cores, cores)
+    _, t = ref.lumcolumn(2048, 64, 1)
+    out["c1_shipped_s1_default_split_gflops"] = lu_flops(2048) / t / 1e9
+    ref.set_threads(cores, 1)
+    return out
+
+
 def cpu_reference_gflops(n: int, nb: int, runs: int) -> dict:
-    """The reference's own lumcolumn on the host cores (oracle/_ref), or the
-    oracle restatement if the reference was not compiled."""
+    """The reference's own lumcolumn on the host cores (oracle/_ref): the
+    bounded N = n sample of the workload (shipped build, the baseline of
+    record; the pivot-fixed build beside it) and BASELINE config 1 (c1_*)."""
     cores = os.cpu_count() or 1
     from oracle.oracle import OracleLib, RefLib
 
-    if RefLib.available("shipped"):
+    if RefLib.available("shipped") and RefLib.available("fixed"):
         ref = RefLib("shipped")
         ref.set_threads(cores, 1)
-        ref.lumcolumn(2048, 64, 1)  # untimed: BLAS threads started, code paged in
-        ts = []
-        for _ in range(runs):
-            _, t = ref.lumcolumn(n, nb, 1)
-            ts.append(t)
-        t = statistics.median(ts)
-        return {"value": lu_flops(n) / t / 1e9, "unit": UNIT, "cores": cores, "kind": "reference",
-                "sample": "lu2 lumcolumn (lu2.c:1122) compiled from the reference sources + OpenBLAS 0.3.15, "
-                          "N=%d nb=%d seed 1, %d OpenBLAS threads, median of %d after an untimed N=2048 "
-                          "run" % (n, nb, cores, runs),
-                "seconds": ts}
+        r = ref_run(ref, n, nb, 1, runs)
+        fixed = RefLib("fixed")
+        fixed.set_threads(cores, 1)
+        rf = ref_run(fixed, n, nb, 1, runs)
+        out = {"value": r["gflops"], "unit": UNIT, "cores": cores, "kind": "reference",
+               "sample": "lu2 lumcolumn (lu2.c:1122) compiled from the reference sources + OpenBLAS 0.3.15, "
+                         "N=%d nb=%d seed 1, OpenBLAS %d threads, 1 OpenMP thread, median of %d after an untimed "
+                         "run; c1_*: N=2048 nb=64 median of 5" % (n, nb, cores, runs),
+               "cpu": cpu_model(), "fixed_gflops": rf["gflops"]}
+        out.update(c1_baseline(cores))
+        return out
     orc = OracleLib()
     n2 = 2048
     a = orc.randomsetmat(n2, 1)
     t0 = time.perf_counter()
     orc.lumcolumn(a, n2, 64)
     t = time.perf_counter() - t0
-    return {"value": lu_flops(n2) / t / 1e9, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": "oracle restatement N=%d nb=64" % n2}
+    return {"value": lu_flops(n2) / t / 1e9, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": "oracle restatement N=%d nb=64" % n2, "cpu": cpu_model()}
 
 
 def fp64_peak(device) -> float:
@@ -330,6 +379,79 @@ def run_batched(ctx, dev, stream, args, max_over_ranks, world, rank=0) -> dict:
             "speedup_vs_loop": sps / (world / t_loop), "fp32_lu_fp64_ir": fp32_ir}
 
 
+def run_swap_profile(ctx, n, nb, dev, stream, reps=5) -> dict:
+    """The top-level row exchange of the first panel (lu2.c:541-554): pivots of
+    rows 0..nb-1 drawn uniformly from the rows below (as partial pivoting on a
+    random matrix picks them) applied to columns nb..n of the order-n matrix.
+    Algorithmic bytes: every row the exchanges touch is read once and written
+    once over the width."""
+    import numpy as np
+    import torch
+
+    ld = n + 16
+    a = torch.empty((n, ld), dtype=torch.float64, device=dev)
+    ctx.generate(a, n, ld, 1)
+    rng = np.random.default_rng(1)
+    piv = np.array([rng.integers(k, n) for k in range(nb)], dtype=np.int32)
+    touched = len(set(range(nb)) | set(int(p) for p in piv))
+    dpiv = torch.tensor(np.concatenate([piv, np.arange(nb, n, dtype=np.int32)]), device=dev)
+    dinv = torch.full((n,), 1.0, dtype=torch.float64, device=dev)
+    width = n + 1 - nb
+    for _ in range(2):
+        ctx.swaprows(a, n, ld, 0, nb, dpiv, dinv, nb, n + 1)
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(reps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ctx.swaprows(a, n, ld, 0, nb, dpiv, dinv, nb, n + 1)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1) / 1e3)
+    t = statistics.median(ts)
+    moved = 2.0 * 8 * touched * width
+    return {"profile_swap": {"n": n, "nb": nb, "rows_touched": touched, "width": width, "seconds": t,
+                             "algorithmic_bytes": moved, "gbs": moved / t / 1e9}}
+
+
+def headline(value, hplres, e2e, roofline, forms) -> dict:
+    """The figures of every form in one short object, printed last on the line."""
+    h = {"fp64_gflops": round(value, 1), "fp64_hpl": hplres, "dgemm_frac_of_cublas": round(roofline["frac"], 4)}
+    if e2e:
+        h["e2e_pinned_gflops"] = round(e2e["value"], 1)
+        if "pageable_value" in e2e:
+            h["e2e_pageable_gflops"] = round(e2e["pageable_value"], 1)
+    m = forms.get("bf16_ir")
+    if m:
+        h.update({"bf16_ir_gflops": round(m["value"], 1), "bf16_ir_speedup_vs_fp64": round(m["speedup_vs_fp64_plain"], 3),
+                  "bf16_ir_iterations": m["iterations"], "bf16_ir_hpl": m["hpl_residual"],
+                  "bf16_ir_x_err_vs_fp64": m["x_rel_err_vs_fp64_lu"]})
+    f = forms.get("fp8_gmres_ir")
+    if f:
+        dd = [v for k, v in f.items() if k.startswith("diagonally_dominant_n")]
+        gen = [v for k, v in f.items() if k.startswith("general_n")]
+        chk = [v for k, v in f.items() if k.startswith("check_n")]
+        if dd:
+            h.update({"fp8_dd_gflops": round(dd[0]["value"], 1), "fp8_dd_gmres_iters": dd[0]["gmres_iterations"],
+                      "fp8_dd_hpl": dd[0]["hpl_residual"]})
+        if gen:
+            h.update({"fp8_general_converged": gen[0]["converged"], "fp8_general_hpl": gen[0]["hpl_residual"]})
+        if chk:
+            h["fp8_fwd_err_dd"] = chk[0]["diagonally_dominant"]["fwd_err_vs_fp64"]
+            h["fp8_fwd_err_general"] = chk[0]["general"]["fwd_err_vs_fp64"]
+    b = forms.get("batched_fp64")
+    if b:
+        h.update({"batched_fp64_systems_s": round(b["value"]), "batched_fp64_max_hpl": b["max_hpl_residual"],
+                  "batched_speedup_vs_loop": round(b["speedup_vs_loop"], 1),
+                  "batched_fp32ir_systems_s": round(b["fp32_lu_fp64_ir"]["value"]),
+                  "batched_fp32ir_max_hpl": b["fp32_lu_fp64_ir"]["max_hpl_residual"]})
+    d = forms.get("host_dgemm")
+    if d:
+        h["host_dgemm_overlap_speedup"] = round(d["speedup"], 3)
+    return h
+
+
 def fp8_update_bytes(n: int, nb: int) -> float:
     """Algorithmic HBM bytes of the FP8 trailing updates of an order-n factorization:
     FP32 C read and written (8 B per element) plus the E4M3 operands (1 B each)."""
@@ -486,6 +608,7 @@ def run_reference(args, rank: int) -> None:
     if not RefLib.available("shipped"):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (the compiled reference) not present"}))
         return
+    c1 = c1_baseline(cores)
     ref = RefLib("shipped")
     ref.set_threads(cores, 1)
     for _ in range(args.warmup):
@@ -503,7 +626,8 @@ def run_reference(args, rank: int) -> None:
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
            "config": {"workload": "plain FP64 LU+solve (reference CPU lu2), N=%d sample of N=%d, nb=%d" %
                                   (n, args.n, nb), "n": n, "nb": nb, "seed": 1},
-           "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
+           "cpu_baseline": dict({"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample,
+                                 "cpu": cpu_model()}, **c1),
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
 
@@ -518,6 +642,8 @@ def main() -> int:
     ap.add_argument("--nb", type=int, default=256)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-e2e-pageable", action="store_true",
+                    help="skip lumcolumn on pageable host memory (one untimed + one timed step)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the BF16-LU + IR measurement")
     ap.add_argument("--mixed-nb", type=int, default=256)
@@ -532,6 +658,9 @@ def main() -> int:
                     help="profiling run for ncu: one FP8-LU + GMRES-IR solve of the diagonally dominant system")
     ap.add_argument("--profile-batched", action="store_true",
                     help="profiling run for ncu: one FP64 batched solve of the batch-count systems")
+    ap.add_argument("--profile-swap", action="store_true",
+                    help="row exchange alone: one panel's pivots (nb random rows below the panel) applied to the "
+                         "full width of the order-n matrix through lu2gpu_swaprows_dev, timed with CUDA events")
     ap.add_argument("--batch-ir", action="store_true",
                     help="--profile-batched in the FP32-LU + FP64 IR mode")
     ap.add_argument("--batch-config", default=None,
@@ -605,6 +734,10 @@ def main() -> int:
                           "config": cfg, "zero_pivots": int((info != 0).sum()),
                           "max_hpl_residual": float(b.residuals().max())}))
         b.close()
+        ctx.close()
+        return 0
+    if args.profile_swap:
+        print(json.dumps(run_swap_profile(ctx, n, nb, dev, stream)))
         ctx.close()
         return 0
     ld = L.device_ld(n)
@@ -720,8 +853,31 @@ def main() -> int:
         e2e = {"value": world * len(ts) * lu_flops(n) / te / 1e9, "unit": UNIT,
                "h2d_bytes_per_step": n * (n + 1) * 8, "d2h_bytes_per_step": n * (n + 1) * 8 + n * 8 + nb * 4,
                "steps": len(ts), "api": "lumcolumn() C entry point, pinned host buffers"}
-        lib.lu2gpu_release()
         del host, bvec
+        # the same on pageable host memory, as lu2's main allocates a
+        # (malloc, lu2.c:1261-1262): one copy in before, one copy out after
+        if not args.no_e2e_pageable:
+            hp = np.empty((n, n + 16))
+            bp = np.empty(n)
+            ts = []
+            for it in range(2):
+                hp[...] = pristine.cpu().numpy()  # untimed restore of the input
+                barrier()
+                f0 = torch.cuda.Event(enable_timing=True)
+                f1 = torch.cuda.Event(enable_timing=True)
+                f0.record(stream)
+                rc = L.lumcolumn(hp, bp, nb, pv, L.PIVOT_PARTIAL)
+                f1.record(stream)
+                torch.cuda.synchronize()
+                if rc != 0:
+                    raise RuntimeError("lumcolumn status %d" % rc)
+                if it > 0:
+                    ts.append(f0.elapsed_time(f1) / 1e3)
+            tp = max_over_ranks(sum(ts))
+            e2e["pageable_value"] = world * len(ts) * lu_flops(n) / tp / 1e9
+            e2e["pageable_steps"] = len(ts)
+            del hp, bp
+        lib.lu2gpu_release()
 
     # precision form: BF16-LU + FP64 iterative refinement on the
     # diagonally dominant system of the same order, against this run's FP64 LU
@@ -756,7 +912,8 @@ def main() -> int:
                           "parallelism": "replicas" if world > 1 else "single",
                           "l2": "inputs (%.1f GB) larger than L2, no flush" % (n * ld * 8 / 1e9)},
                "gpu_launches": int(launches), "hpl_residual": hplres, "clocks": clk, "roofline": roofline,
-               "phases_ms": phases, "e2e": e2e, "cpu_baseline": cpu, "forms": forms}
+               "e2e": e2e, "cpu_baseline": cpu, "phases_ms": phases, "forms": forms,
+               "headline": headline(value, hplres, e2e, roofline, forms)}
         print(json.dumps(out))
     ctx.close()
     if world > 1:

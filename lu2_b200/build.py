@@ -55,7 +55,9 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
             sys.stdout.write(r.stdout + r.stderr)
         objs.append(o)
     tmp = LIB + ".tmp"
-    cmd = [nvcc()] + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs
+    # -Bsymbolic: the library's calls to its own exported names (lu2's
+    # function names) bind to its own definitions, never to a caller's
+    cmd = [nvcc()] + ARCH + ["-shared", "-cudart", "static", "-Xlinker", "-Bsymbolic", "-o", tmp] + objs
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("link failed:\n%s%s" % (r.stdout, r.stderr))

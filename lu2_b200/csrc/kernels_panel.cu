@@ -84,11 +84,14 @@ __device__ __forceinline__ void swap_st(T *p, int avail, const T *in)
     }
 }
 
-template <typename T, int V>
-__global__ void __launch_bounds__(SWAP_THREADS) laswp_scale_kernel(T *a, long ld, int nrows, int k0, int k1,
-                                                                   const int *__restrict__ ipiv, int goff,
-                                                                   const T *__restrict__ dinv, int cs, int ce,
-                                                                   int scale, int *status)
+// NS > 0: every thread keeps its NS row segments of a chunk in registers
+// (all NS loads in flight at once, one barrier per chunk, no staging in
+// shared memory; used while the slots fit, nslot <= NS * rows per pass);
+// NS = 0: the chunk is staged in shared memory.
+template <typename T, int V, int NS>
+__global__ void __launch_bounds__(SWAP_THREADS, NS > 0 ? 2 : 1)
+    laswp_scale_kernel(T *a, long ld, int nrows, int k0, int k1, const int *__restrict__ ipiv, int goff,
+                       const T *__restrict__ dinv, int cs, int ce, int scale, int *status)
 {
     constexpr int COLS = 128 / (int)sizeof(T);  // one 128-byte line of a row per chunk
     constexpr int TPR = COLS / V;               // threads per row segment
@@ -96,8 +99,8 @@ __global__ void __launch_bounds__(SWAP_THREADS) laswp_scale_kernel(T *a, long ld
     constexpr int U = 8;                        // loads in flight per thread
     extern __shared__ __align__(16) unsigned char swap_smem[];
     const int npiv = k1 - k0;
-    T *S = reinterpret_cast<T *>(swap_smem);     // [2 npiv][COLS] staged row segments
-    int *P = reinterpret_cast<int *>(S + (size_t)2 * npiv * COLS);
+    T *S = reinterpret_cast<T *>(swap_smem);     // [2 npiv][COLS] staged row segments (NS = 0)
+    int *P = reinterpret_cast<int *>(S + (NS > 0 ? 0 : (size_t)2 * npiv * COLS));
     int *A = P + npiv;        // chain pointer (>= 0) or root code -(row)-1
     int *src = A + npiv;      // [2 npiv] source row of each slot
     int *dst = src + 2 * npiv; // [2 npiv] destination row of each slot
@@ -175,6 +178,32 @@ __global__ void __launch_bounds__(SWAP_THREADS) laswp_scale_kernel(T *a, long ld
     const int nslot = s_nslot;
     const int cq = (tid % TPR) * V, r0 = tid / TPR;
     const int nchunk = (ce - cs + COLS - 1) / COLS;
+    if constexpr (NS > 0) {
+        for (int chunk = blockIdx.x; chunk < nchunk; chunk += gridDim.x) {
+            const int j = cs + chunk * COLS + cq;
+            const int avail = ce - j;
+            T v[NS][V];
+#pragma unroll
+            for (int u = 0; u < NS; u++) {
+                const int s = r0 + u * RPP;
+                if (s < nslot && avail > 0) swap_ld<T, V>(a + (size_t)src[s] * ld + j, avail, v[u]);
+            }
+            __syncthreads();  // every gather of this chunk's columns precedes every scatter to them
+#pragma unroll
+            for (int u = 0; u < NS; u++) {
+                const int s = r0 + u * RPP;
+                if (s < nslot && avail > 0) {
+                    if (scale && s < npiv) {
+                        const T d = __ldg(dinv + k0 + s);
+#pragma unroll
+                        for (int q = 0; q < V; q++) v[u][q] *= d;
+                    }
+                    swap_st<T, V>(a + (size_t)dst[s] * ld + j, avail, v[u]);
+                }
+            }
+        }
+        return;
+    }
     for (int chunk = blockIdx.x; chunk < nchunk; chunk += gridDim.x) {
         const int j = cs + chunk * COLS + cq;
         const int avail = ce - j;
@@ -213,29 +242,41 @@ __global__ void __launch_bounds__(SWAP_THREADS) laswp_scale_kernel(T *a, long ld
     }
 }
 
-template <typename T, int V>
+template <typename T, int V, int NS>
 static cudaError_t launch_laswp_v(T *a, long ld, int nrows, int k0, int k1, const int *ipiv, int goff, const T *dinv,
                                   int cs, int ce, bool scale, int *status, cudaStream_t st)
 {
     constexpr int COLS = 128 / (int)sizeof(T);
     const int npiv = k1 - k0;
-    const size_t smem = (size_t)2 * npiv * COLS * sizeof(T) + (size_t)6 * npiv * sizeof(int);
+    const size_t smem = (NS > 0 ? 0 : (size_t)2 * npiv * COLS * sizeof(T)) + (size_t)6 * npiv * sizeof(int);
     if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(laswp_scale_kernel<T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             200 * 1024);
+        cudaError_t e = cudaFuncSetAttribute(laswp_scale_kernel<T, V, NS>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         if (e != cudaSuccess) return e;
     }
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    int per_sm = (int)((220 * 1024) / (smem + 1024));
+    int per_sm = NS > 0 ? 2 : (int)((220 * 1024) / (smem + 1024));
     per_sm = per_sm < 1 ? 1 : (per_sm > 4 ? 4 : per_sm);
     int blocks = (ce - cs + COLS - 1) / COLS;
     if (blocks > per_sm * sms) blocks = per_sm * sms;
     count_launch();
-    laswp_scale_kernel<T, V><<<blocks, SWAP_THREADS, smem, st>>>(a, ld, nrows, k0, k1, ipiv, goff, dinv, cs, ce,
-                                                                  scale ? 1 : 0, status);
+    laswp_scale_kernel<T, V, NS><<<blocks, SWAP_THREADS, smem, st>>>(a, ld, nrows, k0, k1, ipiv, goff, dinv, cs,
+                                                                      ce, scale ? 1 : 0, status);
     return cudaGetLastError();
+}
+
+// registers while 2 npiv slots fit NS passes of SWAP_THREADS / (COLS / V) rows
+template <typename T, int V>
+static cudaError_t launch_laswp_pick(T *a, long ld, int nrows, int k0, int k1, const int *ipiv, int goff,
+                                     const T *dinv, int cs, int ce, bool scale, int *status, cudaStream_t st)
+{
+    constexpr int RPP = SWAP_THREADS / ((128 / (int)sizeof(T)) / V);
+    constexpr int NSR = (V > 1) ? 16 : 0;  // 16 passes: 512 slots (npiv <= 256) at 16-byte accesses
+    if (NSR > 0 && 2 * (k1 - k0) <= NSR * RPP)
+        return launch_laswp_v<T, V, NSR>(a, ld, nrows, k0, k1, ipiv, goff, dinv, cs, ce, scale, status, st);
+    return launch_laswp_v<T, V, 0>(a, ld, nrows, k0, k1, ipiv, goff, dinv, cs, ce, scale, status, st);
 }
 
 template <typename T>
@@ -247,8 +288,8 @@ static cudaError_t launch_laswp_scale_t(T *a, long ld, int nrows, int k0, int k1
     constexpr int VW = 16 / (int)sizeof(T);
     // 16-byte accesses when every row segment starts on a 16-byte boundary
     if ((reinterpret_cast<uintptr_t>(a) & 15) == 0 && ld % VW == 0 && cs % VW == 0)
-        return launch_laswp_v<T, VW>(a, ld, nrows, k0, k1, ipiv, goff, dinv, cs, ce, scale, status, st);
-    return launch_laswp_v<T, 1>(a, ld, nrows, k0, k1, ipiv, goff, dinv, cs, ce, scale, status, st);
+        return launch_laswp_pick<T, VW>(a, ld, nrows, k0, k1, ipiv, goff, dinv, cs, ce, scale, status, st);
+    return launch_laswp_pick<T, 1>(a, ld, nrows, k0, k1, ipiv, goff, dinv, cs, ce, scale, status, st);
 }
 
 cudaError_t launch_laswp_scale(double *a, long ld, int nrows, int k0, int k1, const int *ipiv, int goff,

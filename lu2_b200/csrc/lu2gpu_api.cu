@@ -32,6 +32,18 @@ void lu2gpu::count_launch(long k) { g_launches += k; }
 
 extern "C" long lu2gpu_kernel_launches(void) { return g_launches.load(); }
 
+// LU2GPU_REPORT=1: print the number of kernel launches when the process exits
+static void report_at_exit() { fprintf(stderr, "lu2gpu: %ld kernel launches\n", g_launches.load()); }
+
+static void register_report()
+{
+    static std::once_flag once;
+    std::call_once(once, [] {
+        const char *e = getenv("LU2GPU_REPORT");
+        if (e && e[0] == '1') atexit(report_at_exit);
+    });
+}
+
 static void set_error(const char *fmt, ...)
 {
     va_list ap;
@@ -172,6 +184,7 @@ extern "C" int lu2gpu_create(lu2gpu_ctx **out, int device)
         set_error("device %d is sm_%d%d; this library is built for sm_100a only", device, prop.major, prop.minor);
         return LU2GPU_ERR_NODEV;
     }
+    register_report();
     lu2gpu_ctx *c = new lu2gpu_ctx();
     c->device = device;
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {

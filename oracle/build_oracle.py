@@ -113,9 +113,61 @@ def build_ref(verbose: bool = False) -> dict:
         res[name] = so
     with open(os.path.join(OUT_DIR, "BUILD_INFO.txt"), "w") as f:
         f.write("reference: %s\nopenblas: %s\n" % (REF_DIR, blas))
+    if os.path.exists(GPU_LIB):
+        res.update(build_dropin(cflags, objs, lu2o, tlib, blas, verbose))
     if verbose:
         print("built", res)
     return res
+
+
+GPU_LIB = os.path.join(os.path.dirname(HERE), "lu2_b200", "liblu2gpu.so")
+
+
+def build_dropin(cflags: list[str], objs: list[str], lu2o: str, tlib: str, blas: str, verbose: bool) -> dict:
+    """The reference's own programs linked against the GPU library, as a
+    maintainer would link them (no reference source is edited):
+
+    * ``lu2_gdr``: the reference's GDR build (Makefile.common:47-48, 69-70,
+      87-88: lu2.o lu2tlib.o ... lu2lib_gdr.o gdrdgemm.o, lu2lib.c with
+      -DUSEGDR) with liblu2gpu.so in place of the GRAPE-DR library
+      ($(GDRLIBS)): mydgemm sends k > 512 products through mygdrdgemm to the
+      GPU's gdr_dgemm_ (lu2lib.c:2097-2100).
+    * ``libref_lu2_gdr.so``: the same objects with ref_harness.c instead of
+      main, so tests can read its pivots and x.
+    * ``lu2_gpu``: lu2.c's main with lumcolumn from liblu2gpu.so: lu2.c built
+      with -Dlumcolumn=lumcolumn_cpu, that symbol weakened, and
+      dropin_lumcolumn.c's strong lumcolumn_cpu forwarding to the library.
+    """
+    lib_dir = os.path.dirname(GPU_LIB)
+    gdr_lib = os.path.join(OUT_DIR, "lu2lib_gdr.o")
+    _run(["gcc", "-funroll-loops"] + cflags + ["-DUSEGDR", "-c", os.path.join(REF_DIR, "lu2lib.c"), "-o", gdr_lib])
+    gdrdgemm = os.path.join(OUT_DIR, "gdrdgemm.o")
+    _run(["gcc"] + cflags + ["-c", os.path.join(REF_DIR, "gdrdgemm.c"), "-o", gdrdgemm])
+    lu2main = os.path.join(OUT_DIR, "lu2_main.o")
+    _run(["gcc"] + cflags + ["-c", os.path.join(REF_DIR, "lu2.c"), "-o", lu2main])
+    base = [o for o in objs if not o.endswith("lu2lib.o")]  # timerlib, second, lu2_mp_nompi
+    gpu_link = ["-L" + lib_dir, "-llu2gpu", "-Wl,--disable-new-dtags,-rpath,$ORIGIN/../../lu2_b200"]
+    blas_link = [blas, "-Wl,-rpath," + os.path.dirname(blas), "-lpthread", "-lm"]
+    out = {}
+    exe = os.path.join(OUT_DIR, "lu2_gdr")
+    _run(["gcc", "-fopenmp", "-o", exe, lu2main, tlib, gdr_lib, gdrdgemm] + base + gpu_link + blas_link)
+    out["lu2_gdr"] = exe
+    so = os.path.join(OUT_DIR, "libref_lu2_gdr.so")
+    harn = os.path.join(OUT_DIR, "ref_harness.o")
+    _run(["gcc", "-shared", "-fopenmp", "-o", so, harn, lu2o, tlib, gdr_lib, gdrdgemm] + base + gpu_link + blas_link)
+    out["gdr"] = so
+    gpumain = os.path.join(OUT_DIR, "lu2_gpu_main.o")
+    _run(["gcc"] + cflags + ["-Dlumcolumn=lumcolumn_cpu", "-c", os.path.join(REF_DIR, "lu2.c"), "-o", gpumain])
+    _run(["objcopy", "--weaken-symbol=lumcolumn_cpu", gpumain])
+    shim = os.path.join(OUT_DIR, "dropin_lumcolumn.o")
+    _run(["gcc", "-O2", "-fPIC", "-c", os.path.join(HERE, "dropin_lumcolumn.c"), "-o", shim])
+    exe2 = os.path.join(OUT_DIR, "lu2_gpu")
+    lu2lib = [o for o in objs if o.endswith("lu2lib.o")]
+    _run(["gcc", "-fopenmp", "-o", exe2, gpumain, shim, tlib] + lu2lib + base + gpu_link + blas_link)
+    out["lu2_gpu"] = exe2
+    if verbose:
+        print("built", out)
+    return out
 
 
 def main() -> int:

@@ -52,9 +52,15 @@ static double now_s(void)
     return ts.tv_sec + 1e-9 * ts.tv_nsec;
 }
 
+/* thread settings, applied by the worker thread itself: OpenMP's thread
+ * count is a per-thread setting that a new pthread does not inherit */
+static int g_blas_threads = 0, g_omp_threads = 0;
+
 static void *run_job(void *arg)
 {
     job_t *j = (job_t *)arg;
+    if (g_blas_threads > 0) openblas_set_num_threads(g_blas_threads);
+    if (g_omp_threads > 0) omp_set_num_threads(g_omp_threads);
     int n = j->n, nb = j->nb;
     size_t rdim = (size_t)n + 16;
     double *a = malloc(sizeof(double) * (size_t)n * rdim);
@@ -104,11 +110,14 @@ static int run_on_big_stack(job_t *j)
     return j->rc;
 }
 
-/* Threads for OpenBLAS and for the reference's own OpenMP regions. */
+/* Threads for OpenBLAS and for the reference's own OpenMP regions (0: leave
+ * the library default, i.e. all cores unless OMP_NUM_THREADS /
+ * OPENBLAS_NUM_THREADS say otherwise). */
 void ref_set_threads(int blas_threads, int omp_threads)
 {
+    g_blas_threads = blas_threads;
+    g_omp_threads = omp_threads;
     if (blas_threads > 0) openblas_set_num_threads(blas_threads);
-    if (omp_threads > 0) omp_set_num_threads(omp_threads);
 }
 
 /* Per-panel drive of the reference (records the full pivot sequence). */
