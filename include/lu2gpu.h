@@ -339,6 +339,16 @@ long lu2gpu_kernel_launches(void);
  * stays usable.  lu2gpu_test_leaf_withhold(ctx, -1, 0) switches it off. */
 int lu2gpu_test_leaf_withhold(lu2gpu_ctx *ctx, int cta, double wait_ms);
 
+/* lu2.c:485-521 (solve_triangle: U12 = L11^{-1} A12) on the device: x (K x
+ * ncols, row stride ldx) := T^{-1} x, T the unit lower triangle whose strict
+ * lower part is that of the K x K block t (row stride ldt), K <= 512; bt
+ * (device, may be NULL) receives -x^T (ncols x K, K-contiguous), the operand
+ * the trailing update reads.  With K a multiple of 16 up to 256 and 16-byte
+ * aligned operands with even strides it runs on the FP64 tensor pipe.
+ * Synchronous. */
+int lu2gpu_solve_triangle_dev(lu2gpu_ctx *ctx, int K, const double *t, long ldt, double *x, long ldx, int ncols,
+                              double *bt);
+
 /* lu2.c:251-291 (swaprows_simple_with_scale, as lu2.c:541-554 applies a
  * panel's pivots) on the device: for k = k0..k1-1 in order, exchange rows k and
  * ipiv[k] of columns cs..ce-1 of the n-row row-major device matrix a (leading

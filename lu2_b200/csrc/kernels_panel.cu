@@ -7,6 +7,7 @@
 //               lu2.c:1107-1118
 //   trsm        lu2.c:485-521 (solve_triangle: U12 = L11^{-1} A12)
 #include <climits>
+#include <cstdlib>
 
 #include <cuda_bf16.h>
 
@@ -399,6 +400,200 @@ __global__ void __launch_bounds__(256) trsm_unit_lower_kernel(const E *T, long l
     }
 }
 
+// ---------------------------------------------------------------------------
+// FP64 block-row solve on the FP64 tensor pipe (mma.sync m16n8k8 f64), for
+// K a multiple of 16 up to 256.  X := T^{-1} X is done in 16-row blocks b:
+// block b is finished by forward substitution with T's 16x16 unit-lower
+// diagonal block (the CUDA-core solve's order of operations: for l, for r > l,
+// x_r -= t_rl x_l), then X_i -= T_ib X_b for every block i below on the
+// tensor pipe -- the blocked substitution of lu2's solve_triangle
+// (lu2.c:485-521).  Each warp owns 8 columns of X and keeps all K rows of them
+// in registers as MMA accumulators, so no step waits for another warp; T's
+// 16-column block b (rows below the diagonal block) is staged in shared
+// memory per step, double-buffered with cp.async, and shared by the CTA's
+// warps.  Two 4-warp CTAs share an SM, so one CTA's substitutions overlap the
+// other's products.  Outputs: X in place (16-byte stores) and
+// bt[j*K + r] = -X[r][j] written in 128-byte column segments through a
+// per-warp scratch tile.
+constexpr int TD_WARPS = 4;
+constexpr int TD_COLS = 8 * TD_WARPS;  // columns of X per CTA
+constexpr int TD_MAXB = 16;            // K <= 256
+constexpr int TD_TP = 18;              // padded pitch (doubles): fragment rows g, g+4 in opposite bank halves
+constexpr int TD_SP = 9;               // pitch of the per-warp 16 x 8 scratch tile
+constexpr int TD_TROWS = 16 * TD_MAXB - 16;  // rows of a staged T block (below the diagonal block)
+constexpr size_t TD_SMEM =
+    (size_t)(2 * TD_TROWS * TD_TP + TD_MAXB * 16 * TD_TP + TD_WARPS * 16 * TD_SP) * sizeof(double);
+
+__device__ __forceinline__ void td_mma(double (&c)[4], double a0, double a1, double a2, double a3, double b0, double b1)
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+        : "d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(b0), "d"(b1));
+}
+
+__device__ __forceinline__ void td_cp16(void *dst, const void *src)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+                 "l"(src)
+                 : "memory");
+}
+
+__global__ void __launch_bounds__(TD_WARPS * 32, 2)
+    trsm_dmma_kernel(const double *__restrict__ T, long ldt, double *X, long ldx, int K, int ncols, double *bt)
+{
+    extern __shared__ __align__(16) double td_smem[];
+    double *Tb = td_smem;                  // [2][TD_TROWS][TD_TP]
+    double *Lv = Tb + 2 * TD_TROWS * TD_TP;  // [TD_MAXB][16][TD_TP]: the diagonal blocks, strict lower part
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int g = lane >> 2, t = lane & 3;
+    double *S = Lv + TD_MAXB * 16 * TD_TP + warp * 16 * TD_SP;  // this warp's 16 x 8 tile
+    const int nbk = K >> 4;
+    const int c0 = blockIdx.x * TD_COLS + warp * 8;
+
+    // T's column block b, rows 16(b+1)..K-1, into Tb[b & 1] (row r of the
+    // block at row r - 16(b+1)); 16-byte copies, 8 per row
+    auto stage = [&](int b) {
+        double *dst = Tb + (b & 1) * TD_TROWS * TD_TP;
+        const int rows = K - 16 * (b + 1);
+        for (int q = tid; q < rows * 8; q += TD_WARPS * 32) {
+            const int r = q >> 3, ch = q & 7;
+            td_cp16(dst + r * TD_TP + 2 * ch, T + (size_t)(16 * (b + 1) + r) * ldt + 16 * b + 2 * ch);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    stage(0);
+    for (int q = tid; q < nbk * 256; q += TD_WARPS * 32) {
+        const int b = q >> 8, r = (q >> 4) & 15, c = q & 15;
+        Lv[(b * 16 + r) * TD_TP + c] = (c < r) ? T[(size_t)(16 * b + r) * ldt + 16 * b + c] : 0.0;
+    }
+
+    // this warp's columns of X as accumulators: block i, rows 16i+g and
+    // 16i+g+8, columns c0+2t and c0+2t+1
+    const int col = c0 + 2 * t;
+    const bool c_ok0 = col < ncols, c_ok1 = col + 1 < ncols;
+    // 16-byte accesses to X where its rows allow them
+    const bool xvec = ((reinterpret_cast<uintptr_t>(X) & 15) == 0) && ((ldx & 1) == 0);
+    double acc[TD_MAXB][4];
+#pragma unroll
+    for (int i = 0; i < TD_MAXB; i++) {
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            double v0 = 0.0, v1 = 0.0;
+            if (i < nbk) {
+                const double *p = X + (size_t)(16 * i + g + 8 * h) * ldx + col;
+                if (c_ok1 && xvec) {
+                    const double2 w = *reinterpret_cast<const double2 *>(p);
+                    v0 = w.x;
+                    v1 = w.y;
+                } else {
+                    if (c_ok0) v0 = p[0];
+                    if (c_ok1) v1 = p[1];
+                }
+            }
+            acc[i][2 * h] = v0;
+            acc[i][2 * h + 1] = v1;
+        }
+    }
+
+#pragma unroll
+    for (int b = 0; b < TD_MAXB; b++) {
+        if (b >= nbk) break;
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
+        __syncthreads();  // Tb[b & 1] (and at b = 0 the diagonal blocks) visible; step b-1's readers of Tb[(b+1) & 1] done
+        if (b + 1 < nbk) stage(b + 1);
+        // block b by forward substitution, one lane per column, through the scratch tile
+        S[g * TD_SP + 2 * t] = acc[b][0];
+        S[g * TD_SP + 2 * t + 1] = acc[b][1];
+        S[(g + 8) * TD_SP + 2 * t] = acc[b][2];
+        S[(g + 8) * TD_SP + 2 * t + 1] = acc[b][3];
+        __syncwarp();
+        if (lane < 8) {
+            const double *Lb = Lv + b * 16 * TD_TP;
+            double xd[16];
+#pragma unroll
+            for (int r = 0; r < 16; r++) xd[r] = S[r * TD_SP + lane];
+#pragma unroll
+            for (int l = 0; l < 15; l++)
+#pragma unroll
+                for (int r = l + 1; r < 16; r++) xd[r] -= Lb[r * TD_TP + l] * xd[l];
+#pragma unroll
+            for (int r = 0; r < 16; r++) S[r * TD_SP + lane] = xd[r];
+        }
+        __syncwarp();
+        // final rows 16b.. of X, and -X^T into bt (column j = lane / 4, rows 4(lane % 4)..+3)
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const double x0 = S[(g + 8 * h) * TD_SP + 2 * t], x1 = S[(g + 8 * h) * TD_SP + 2 * t + 1];
+            double *p = X + (size_t)(16 * b + g + 8 * h) * ldx + col;
+            if (c_ok1 && xvec) {
+                *reinterpret_cast<double2 *>(p) = make_double2(x0, x1);
+            } else {
+                if (c_ok0) p[0] = x0;
+                if (c_ok1) p[1] = x1;
+            }
+        }
+        if (bt) {
+            const int j = lane >> 2, q = lane & 3;
+            if (c0 + j < ncols) {
+                double *p = bt + (size_t)(c0 + j) * K + 16 * b + 4 * q;
+                *reinterpret_cast<double2 *>(p) = make_double2(-S[(4 * q) * TD_SP + j], -S[(4 * q + 1) * TD_SP + j]);
+                *reinterpret_cast<double2 *>(p + 2) =
+                    make_double2(-S[(4 * q + 2) * TD_SP + j], -S[(4 * q + 3) * TD_SP + j]);
+            }
+        }
+        // X_b as the operand of the updates below
+        double bb[2][2];
+#pragma unroll
+        for (int kk = 0; kk < 2; kk++) {
+            bb[kk][0] = S[(8 * kk + t) * TD_SP + g];
+            bb[kk][1] = S[(8 * kk + t + 4) * TD_SP + g];
+        }
+        __syncwarp();  // the scratch is rewritten at the next step
+        const double *Tc = Tb + (b & 1) * TD_TROWS * TD_TP;
+#pragma unroll
+        for (int i = 0; i < TD_MAXB; i++) {
+            if (i <= b || i >= nbk) continue;
+            // s = T_ib X_b from zero, then X_i -= s: the CUDA-core solve's rounding structure
+            const double *A = Tc + (16 * (i - b - 1)) * TD_TP;
+            double sum[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+            for (int kk = 0; kk < 2; kk++)
+                td_mma(sum, A[g * TD_TP + 8 * kk + t], A[(g + 8) * TD_TP + 8 * kk + t], A[g * TD_TP + 8 * kk + t + 4],
+                       A[(g + 8) * TD_TP + 8 * kk + t + 4], bb[kk][0], bb[kk][1]);
+#pragma unroll
+            for (int q = 0; q < 4; q++) acc[i][q] -= sum[q];
+        }
+    }
+}
+
+// the tensor-pipe solve when its layout conditions hold (K a multiple of 16
+// up to 256; T and bt 16-byte aligned, T's stride even), else the CUDA-core
+// one.  The choice never depends on the number of columns: each column's
+// result depends only on T and that column, so a schedule that solves a
+// column group on its own gets the same bits as one that solves it as part of
+// a wider block.
+static bool trsm_dmma_ok(const double *t, long ldt, const double *x, long ldx, int K, int ncols, const double *bt)
+{
+    if (K <= 0 || K > 16 * TD_MAXB || (K & 15) || ncols <= 0) return false;
+    if ((reinterpret_cast<uintptr_t>(t) & 15) || (ldt & 1)) return false;  // cp.async of T's rows
+    if (reinterpret_cast<uintptr_t>(x) & 7) return false;
+    if (bt && (reinterpret_cast<uintptr_t>(bt) & 15)) return false;
+    return true;
+}
+
+static cudaError_t launch_trsm_dmma(const double *t, long ldt, double *x, long ldx, int K, int ncols, double *bt,
+                                    cudaStream_t st)
+{
+    cudaError_t e = cudaFuncSetAttribute(trsm_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TD_SMEM);
+    if (e != cudaSuccess) return e;
+    const int blocks = (ncols + TD_COLS - 1) / TD_COLS;
+    count_launch();
+    trsm_dmma_kernel<<<blocks, TD_WARPS * 32, TD_SMEM, st>>>(t, ldt, x, ldx, K, ncols, bt);
+    return cudaGetLastError();
+}
+
 template <typename E, typename BT>
 static cudaError_t launch_trsm_t(const E *t, long ldt, E *x, long ldx, int K, int ncols, BT *bt, const float *bt_scale, int bt_neg,
                                  cudaStream_t st)
@@ -420,6 +615,13 @@ static cudaError_t launch_trsm_t(const E *t, long ldt, E *x, long ldx, int K, in
 cudaError_t launch_trsm_unit_lower_tx(const double *t, long ldt, double *x, long ldx, int K, int ncols, double *bt,
                                       cudaStream_t st)
 {
+    if (ncols <= 0 || K <= 0) return cudaSuccess;
+    static int use_dmma = -1;  // LU2GPU_TRSM_DMMA=0 selects the CUDA-core solve everywhere (A/B checks)
+    if (use_dmma < 0) {
+        const char *e = getenv("LU2GPU_TRSM_DMMA");
+        use_dmma = (e && e[0] == '0') ? 0 : 1;
+    }
+    if (use_dmma && trsm_dmma_ok(t, ldt, x, ldx, K, ncols, bt)) return launch_trsm_dmma(t, ldt, x, ldx, K, ncols, bt, st);
     return launch_trsm_t<double, double>(t, ldt, x, ldx, K, ncols, bt, nullptr, 1, st);
 }
 

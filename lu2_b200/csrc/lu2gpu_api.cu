@@ -836,6 +836,22 @@ extern "C" int lu2gpu_dgemm_dev(lu2gpu_ctx *c, int m, int n, int k, double alpha
     return end_status(c, "lu2gpu_dgemm_dev");
 }
 
+// lu2.c:485-521 on device memory
+extern "C" int lu2gpu_solve_triangle_dev(lu2gpu_ctx *c, int K, const double *t, long ldt, double *x, long ldx,
+                                         int ncols, double *bt)
+{
+    if (!c || K <= 0 || K > NB_MAX || !t || ldt < K || !x || ncols < 0 || (ncols > 0 && ldx < ncols)) {
+        set_error("lu2gpu_solve_triangle_dev: bad arguments");
+        return LU2GPU_ERR_ARG;
+    }
+    if (ncols == 0) return 0;
+    DeviceGuard g(c->device);
+    int rc = begin_status(c);
+    if (rc) return rc;
+    K_TRY(launch_trsm_unit_lower_tx(t, ldt, x, ldx, K, ncols, bt, c->stream));
+    return end_status(c, "lu2gpu_solve_triangle_dev");
+}
+
 // lu2.c:251-291 over a panel's pivots, as lu2.c:541-554 applies them
 extern "C" int lu2gpu_swaprows_dev(lu2gpu_ctx *c, int n, double *a, long lda, int k0, int k1, const int *ipiv,
                                    const double *dinv, int cs, int ce)

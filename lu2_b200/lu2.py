@@ -211,6 +211,12 @@ class Context:
         _check("lu2gpu_swaprows_dev", lib().lu2gpu_swaprows_dev(self._h, n, _ptr(a), lda, k0, k1, _ptr(ipiv),
                                                                  _ptr(dinv) if dinv is not None else None, cs, ce))
 
+    def solve_triangle(self, K: int, t, ldt: int, x, ldx: int, ncols: int, bt=None) -> None:
+        """x := T^{-1} x with T the unit lower triangle of the K x K block t;
+        bt (optional) receives -x^T (lu2.c:485-521 on device memory)."""
+        _check("lu2gpu_solve_triangle_dev", lib().lu2gpu_solve_triangle_dev(self._h, K, _ptr(t), ldt, _ptr(x), ldx,
+                                                                             ncols, _ptr(bt) if bt is not None else None))
+
     def test_leaf_withhold(self, cta: int, wait_ms: float) -> None:
         """Fault-path test hook: leaf waits give up after wait_ms; CTA `cta` skips its publications."""
         _check("lu2gpu_test_leaf_withhold", lib().lu2gpu_test_leaf_withhold(self._h, cta, wait_ms))

@@ -22,7 +22,7 @@ def _p(x):
                           (2048, 256, 1, "fixed", L.PIVOT_PARTIAL),
                           (256, 64, 12345, "shipped", L.PIVOT_REF)])
 def test_lu2_panel_loop_through_boundary(oracle, golden, parity, n, nb, seed, variant, mode):
-    """Bars as in test_gpu_lu.py: max(1e-12, 2 d_ref) against the fixed
+    """Bars as in test_gpu_lu.py: max(1e-12, 4 d_ref) against the fixed
     reference, 4 d_ref against the shipped one (d_ref = that reference's own
     forward error against the extended-precision solution)."""
     lib = L.load()
@@ -44,7 +44,7 @@ def test_lu2_panel_loop_through_boundary(oracle, golden, parity, n, nb, seed, va
     xr = golden[key + "_x"]
     xhp = golden["hp_n%d_s%d_x" % (n, seed)]
     d_ref = np.abs(xr - xhp).max() / np.abs(xhp).max()
-    bar = max(1e-12, 2 * d_ref) if mode == L.PIVOT_PARTIAL else 4 * d_ref
+    bar = max(1e-12, 4 * d_ref) if mode == L.PIVOT_PARTIAL else 4 * d_ref
     parity("lu2 panel loop %s n=%d nb=%d seed=%d" % (variant, n, nb, seed), np.abs(b - xr).max() / np.abs(xr).max(),
            bar, "fwd err ref %.2e" % d_ref)
 

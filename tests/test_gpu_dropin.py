@@ -51,12 +51,19 @@ def test_lu2_main_runs_the_library_lumcolumn(oracle):
 
 
 def test_lu2_main_reference_pivoting_through_the_environment(oracle):
+    """LU2GPU_PIVOT=ref reaches the library through lu2's unchanged main: the
+    bug-compatible pivots (lu2tlib.c:1052) raise Emax far above the
+    partial-pivoting run's, and it stays below the shipped CPU build's own
+    (same pivots; that build also inverts L11 explicitly, lu2.c:370-483,
+    which amplifies the large multipliers those pivots produce)."""
     n, nb = 4096, 2048
     emax, launches, _, _ = run_program("lu2_gpu", "-n %d -b %d -s 1" % (n, nb), {"LU2GPU_PIVOT": "ref"})
+    e_partial, _, _, _ = run_program("lu2_gpu", "-n %d -b %d -s 1" % (n, nb))
     e_shipped, _, _ = cpu_emax("shipped", n, nb, 1, oracle)
-    print("lu2_gpu LU2GPU_PIVOT=ref: Emax %.3e (shipped CPU reference %.3e)" % (emax, e_shipped))
+    print("lu2_gpu LU2GPU_PIVOT=ref: Emax %.3e (partial pivoting %.3e, shipped CPU reference %.3e)"
+          % (emax, e_partial, e_shipped))
     assert launches > 1000
-    assert e_shipped / 10 < emax < 10 * e_shipped
+    assert 10 * e_partial < emax < 10 * e_shipped
 
 
 def test_lu2_gdr_build_with_the_gpu_as_its_board(oracle):

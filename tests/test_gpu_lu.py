@@ -9,12 +9,15 @@ Bars.  Pivots: equal index for index.  x, relative in the max norm:
   on the diagonally dominant systems.  On lu2's uniform random matrices two
   correct FP64 LUs already differ by more at n = 2048 (cond ~ 4e5; the fixed
   reference and LAPACK differ by up to 1.3e-12), so there the bar is
-  max(XTOL_PARTIAL, 2 d_ref), d_ref being the reference's own forward error
-  against the extended-precision solution: a solver as accurate as the
-  reference is within 2 d_ref of it (triangle inequality).
-* the bug-compatible mode against the shipped reference: 4 d_ref.  That
-  algorithm's poor pivots make its rounding error large (1e-12 .. 1e-8), and
-  two evaluation orders differ by about that error.
+  max(XTOL_PARTIAL, REF_FACTOR d_ref), d_ref being the reference's own
+  forward error against the extended-precision solution.  Forward errors of
+  correct FP64 LUs of one system scatter by up to about 3x either way
+  (LAPACK 0.45-1x the fixed reference's; this repository's C restatement up
+  to 2.96x), and a solver whose forward error is at most 3 d_ref lies within
+  4 d_ref of the reference (triangle inequality).
+* the bug-compatible mode against the shipped reference: REF_FACTOR d_ref as
+  well.  That algorithm's poor pivots make its rounding error large
+  (1e-12 .. 1e-8), and two evaluation orders differ by about that error.
 
 The GPU's own forward error is reported beside each case.  HPL scaled
 residual < 16 in partial-pivoting mode."""
@@ -40,7 +43,7 @@ def rel(x, y):
 def x_bar(mode, d_ref):
     """The bar for x against the reference variant matching `mode`, whose
     forward error is d_ref."""
-    return max(XTOL_PARTIAL, 2.0 * d_ref) if mode == PIVOT_PARTIAL else REF_FACTOR * d_ref
+    return max(XTOL_PARTIAL, REF_FACTOR * d_ref) if mode == PIVOT_PARTIAL else REF_FACTOR * d_ref
 
 
 def dev_matrix(ctx, n, seed, nrhs=1, kind=0):
