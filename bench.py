@@ -379,40 +379,108 @@ def run_batched(ctx, dev, stream, args, max_over_ranks, world, rank=0) -> dict:
             "speedup_vs_loop": sps / (world / t_loop), "fp32_lu_fp64_ir": fp32_ir}
 
 
-def run_swap_profile(ctx, n, nb, dev, stream, reps=5) -> dict:
-    """The top-level row exchange of the first panel (lu2.c:541-554): pivots of
-    rows 0..nb-1 drawn uniformly from the rows below (as partial pivoting on a
-    random matrix picks them) applied to columns nb..n of the order-n matrix.
-    Algorithmic bytes: every row the exchanges touch is read once and written
-    once over the width."""
-    import numpy as np
+def event_median(fn, stream, reps=5, warm=2) -> float:
+    """median CUDA-event seconds of fn() on `stream` after `warm` untimed calls"""
     import torch
 
-    ld = n + 16
-    a = torch.empty((n, ld), dtype=torch.float64, device=dev)
-    ctx.generate(a, n, ld, 1)
-    rng = np.random.default_rng(1)
-    piv = np.array([rng.integers(k, n) for k in range(nb)], dtype=np.int32)
-    touched = len(set(range(nb)) | set(int(p) for p in piv))
-    dpiv = torch.tensor(np.concatenate([piv, np.arange(nb, n, dtype=np.int32)]), device=dev)
-    dinv = torch.full((n,), 1.0, dtype=torch.float64, device=dev)
-    width = n + 1 - nb
-    for _ in range(2):
-        ctx.swaprows(a, n, ld, 0, nb, dpiv, dinv, nb, n + 1)
+    for _ in range(warm):
+        fn()
     torch.cuda.synchronize()
     ts = []
     for _ in range(reps):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        ctx.swaprows(a, n, ld, 0, nb, dpiv, dinv, nb, n + 1)
+        fn()
         e1.record(stream)
         torch.cuda.synchronize()
         ts.append(e0.elapsed_time(e1) / 1e3)
-    t = statistics.median(ts)
+    return statistics.median(ts)
+
+
+def run_swap_profile(ctx, n, nb, dev, stream, rows=None, reps=5) -> dict:
+    """The top-level row exchange of the first panel (lu2.c:541-554): pivots of
+    rows 0..nb-1 drawn uniformly from the rows below (as partial pivoting on a
+    random matrix picks them) applied to columns nb..n of a matrix of `rows`
+    rows (default n) and row stride n+16.  Algorithmic bytes: every row the
+    exchanges touch is read once and written once over the width."""
+    import numpy as np
+    import torch
+
+    rows = rows or n
+    ld = n + 16
+    a = torch.empty((rows, ld), dtype=torch.float64, device=dev)
+    a.uniform_(-0.5, 0.5)
+    rng = np.random.default_rng(1)
+    piv = np.array([rng.integers(k, rows) for k in range(nb)], dtype=np.int32)
+    touched = len(set(range(nb)) | set(int(p) for p in piv))
+    dpiv = torch.tensor(piv, device=dev)
+    dinv = torch.full((nb,), 1.0, dtype=torch.float64, device=dev)
+    width = n + 1 - nb
+    t = event_median(lambda: ctx.swaprows(a, rows, ld, 0, nb, dpiv, dinv, nb, n + 1), stream, reps)
     moved = 2.0 * 8 * touched * width
-    return {"profile_swap": {"n": n, "nb": nb, "rows_touched": touched, "width": width, "seconds": t,
+    return {"profile_swap": {"n": n, "rows": rows, "nb": nb, "rows_touched": touched, "width": width, "seconds": t,
                              "algorithmic_bytes": moved, "gbs": moved / t / 1e9}}
+
+
+def run_trsm_profile(ctx, n, nb, dev, stream, reps=5) -> dict:
+    """The top-level block-row solve of the first panel (lu2.c:485-521): L11
+    the unit lower triangle of a factored nb x nb panel, X an nb x (n+1-nb)
+    block of the matrix (row stride n+16), -X^T written to a separate buffer.
+    Algorithmic work: nb^2 (n+1-nb) FLOPs (a triangular solve), bytes: X read
+    and written and -X^T written once."""
+    import torch
+
+    import numpy as np
+    import scipy.linalg as sl
+
+    ld = n + 16
+    width = n + 1 - nb
+    # L11 of an LU with partial pivoting (|l| <= 1), factored on the host so
+    # that the only solve launches are the measured ones
+    _, lo, _ = sl.lu(np.random.default_rng(3).uniform(-0.5, 0.5, (nb, nb)))
+    t_host = np.zeros((nb, nb + 16))
+    t_host[:, :nb] = np.tril(lo, -1)
+    t_blk = torch.tensor(t_host, device=dev)
+    x = torch.empty((nb, ld), dtype=torch.float64, device=dev)
+    x.uniform_(-0.5, 0.5)
+    x0 = x.clone()
+    bt = torch.empty((width, nb), dtype=torch.float64, device=dev)
+
+    def fn():
+        x.copy_(x0)
+        ctx.solve_triangle(nb, t_blk, nb + 16, x[:, nb:], ld, width, bt)
+
+    t_copy = event_median(lambda: x.copy_(x0), stream, reps)
+    t = event_median(fn, stream, reps) - t_copy
+    flops = float(nb) * nb * width
+    moved = 3.0 * 8 * nb * width
+    return {"profile_trsm": {"n": n, "nb": nb, "width": width, "seconds": t, "flops": flops,
+                             "tflops": flops / t / 1e12, "algorithmic_bytes": moved, "gbs": moved / t / 1e9}}
+
+
+def run_backsolve_profile(ctx, n, nb, dev, stream, reps=5) -> dict:
+    """backward_sub (lu2.c:110-116) alone on a factored order-n system: the
+    upper triangle (8 n^2 / 2 bytes) read once per solve."""
+    import torch
+
+    import lu2_b200 as L
+
+    ld = L.device_ld(n)
+    a = torch.empty((n, ld), dtype=torch.float64, device=dev)
+    ctx.generate(a, n, ld, 1)
+    if ctx.factor(a, n, ld, nb, 1, L.PIVOT_PARTIAL) != 0:
+        raise RuntimeError("zero pivot")
+    y = a[:, n].clone().reshape(n, 1).contiguous()
+    x = y.clone()
+
+    def fn():
+        x.copy_(y)
+        ctx.backsolve(a, n, ld, x, 1, 1)
+
+    t = event_median(fn, stream, reps) - event_median(lambda: x.copy_(y), stream, reps)
+    moved = 8.0 * n * n / 2
+    return {"profile_backsolve": {"n": n, "seconds": t, "algorithmic_bytes": moved, "gbs": moved / t / 1e9}}
 
 
 def headline(value, hplres, e2e, roofline, forms) -> dict:
@@ -661,6 +729,14 @@ def main() -> int:
     ap.add_argument("--profile-swap", action="store_true",
                     help="row exchange alone: one panel's pivots (nb random rows below the panel) applied to the "
                          "full width of the order-n matrix through lu2gpu_swaprows_dev, timed with CUDA events")
+    ap.add_argument("--swap-rows", type=int, default=0,
+                    help="--profile-swap on a matrix of this many rows (pivots drawn below the panel within them; "
+                         "0: n rows), so a capture of the full width holds a few GB")
+    ap.add_argument("--profile-trsm", action="store_true",
+                    help="block-row solve alone: U12 = L11^-1 A12 for an nb x n block (lu2gpu_solve_triangle_dev, "
+                         "L11 from a real panel), timed with CUDA events")
+    ap.add_argument("--profile-backsolve", action="store_true",
+                    help="back substitution alone: factor the order-n system, then time lu2gpu_backsolve")
     ap.add_argument("--batch-ir", action="store_true",
                     help="--profile-batched in the FP32-LU + FP64 IR mode")
     ap.add_argument("--batch-config", default=None,
@@ -737,7 +813,15 @@ def main() -> int:
         ctx.close()
         return 0
     if args.profile_swap:
-        print(json.dumps(run_swap_profile(ctx, n, nb, dev, stream)))
+        print(json.dumps(run_swap_profile(ctx, n, nb, dev, stream, rows=args.swap_rows or n)))
+        ctx.close()
+        return 0
+    if args.profile_trsm:
+        print(json.dumps(run_trsm_profile(ctx, n, nb, dev, stream)))
+        ctx.close()
+        return 0
+    if args.profile_backsolve:
+        print(json.dumps(run_backsolve_profile(ctx, n, nb, dev, stream)))
         ctx.close()
         return 0
     ld = L.device_ld(n)

@@ -146,14 +146,280 @@ static cudaError_t launch_backsolve_t(const T *a, long ld, int n, int nrhs, T *x
     return cudaGetLastError();
 }
 
-cudaError_t launch_backsolve(const double *a, long ld, int n, int nrhs, double *x, long ldx, cudaStream_t st)
+// ---------------------------------------------------------------------------
+// Persistent back substitution for large n.  Rows are cut into 64-row blocks,
+// counted from the bottom (p = 0 is the last block); block p belongs to CTA
+// p mod G of a cooperative grid of G co-resident CTAs, which keeps the
+// right-hand sides of all its blocks in shared memory.  The blocks' solutions
+// x_p are published in the order p = 0, 1, 2, ...: when x_p is out, every CTA
+// subtracts U(block q, block p) x_p from each of its blocks q > p, in that
+// order, so every element receives its updates in a fixed order; the CTA
+// owning block p+1 does that block first and solves it at once (column
+// oriented, one warp per right-hand side), so the critical path per block is
+// one 64x64 product and one 64x64 solve.  Each block of U is read once.
+// Publication: the block's x rows, then a fence and a release store of the
+// call's epoch into the block's flag; readers acquire the flag (bounded wait)
+// and read x through L2.
+constexpr int BSP = 64;          // rows per block
+constexpr int BSP_THREADS = 256;
+
+template <typename T>
+struct BsParams {
+    const T *a;
+    long ld;
+    int n, nblk;
+    T *x;
+    long ldx;
+    int c0, nr;
+    unsigned *flags;
+    unsigned epoch;
+    int *status;
+};
+
+__device__ __forceinline__ unsigned bs_ld_acquire(const unsigned *p)
 {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void bs_st_release(unsigned *p, unsigned v)
+{
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+template <typename T>
+__global__ void __launch_bounds__(BSP_THREADS) backsolve_persistent_kernel(BsParams<T> P)
+{
+    extern __shared__ __align__(16) unsigned char bsp_smem[];
+    const int G = gridDim.x, cta = blockIdx.x, tid = threadIdx.x;
+    const int nblk = P.nblk, nr = P.nr;
+    const int n_own = cta < nblk ? (nblk - cta + G - 1) / G : 0;
+    T *acc = reinterpret_cast<T *>(bsp_smem);      // [n_own][BSP][BS_MAXR]
+    T *Ud = acc + (size_t)n_own * BSP * BS_MAXR;    // [BSP][BSP + 1]
+    T *xs = Ud + BSP * (BSP + 1);                   // [2][BSP][BS_MAXR]
+    __shared__ int s_fail;
+    // block p covers rows r0(p) .. r0(p) + rows(p) - 1
+    auto r0_of = [&](int p) { return (nblk - 1 - p) * BSP; };
+    auto rows_of = [&](int p) { return min(BSP, P.n - r0_of(p)); };
+
+    if (tid == 0) s_fail = 0;
+    for (int k = 0; k < n_own; k++) {
+        const int p = cta + k * G, r0 = r0_of(p), rows = rows_of(p);
+        for (int e = tid; e < BSP * BS_MAXR; e += BSP_THREADS) {
+            const int r = e / BS_MAXR, q = e % BS_MAXR;
+            acc[((size_t)k * BSP + r) * BS_MAXR + q] = (r < rows && q < nr) ? P.x[(size_t)(r0 + r) * P.ldx + P.c0 + q] : T(0);
+        }
+    }
+    __syncthreads();
+
+    // owned block k's diagonal tile into Ud, asynchronously (issued right after
+    // the previous solve, so the copy is off the critical path); only the
+    // strict upper part of the first `rows` rows and columns is read later
+    auto prefetch_diag = [&](int k) {
+        const int p = cta + k * G, r0 = r0_of(p), rows = rows_of(p);
+        for (int e = tid; e < BSP * BSP; e += BSP_THREADS) {
+            const int r = e / BSP, c = e % BSP;
+            if (r < rows && c < rows && c > r) {
+                const unsigned dst = (unsigned)__cvta_generic_to_shared(&Ud[r * (BSP + 1) + c]);
+                if constexpr (sizeof(T) == 8)
+                    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst),
+                                 "l"(P.a + (size_t)(r0 + r) * P.ld + r0 + c)
+                                 : "memory");
+                else
+                    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst),
+                                 "l"(P.a + (size_t)(r0 + r) * P.ld + r0 + c)
+                                 : "memory");
+            }
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+
+    // solve owned block k (all updates from the blocks below applied) into xs[buf] and x; publish
+    auto solve = [&](int k, int buf) {
+        const int p = cta + k * G, r0 = r0_of(p), rows = rows_of(p);
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
+        __syncthreads();
+        const int warp = tid >> 5, lane = tid & 31;
+        T *A = acc + (size_t)k * BSP * BS_MAXR;
+        if (warp < nr) {
+            T y0 = A[lane * BS_MAXR + warp], y1 = A[(lane + 32) * BS_MAXR + warp];
+            for (int c = rows - 1; c >= 0; c--) {  // x_c final: rows above subtract U'[r][c] x_c
+                const T xc = __shfl_sync(0xffffffffu, c >= 32 ? y1 : y0, c & 31);
+                if (lane < c) y0 -= Ud[lane * (BSP + 1) + c] * xc;
+                if (lane + 32 < c) y1 -= Ud[(lane + 32) * (BSP + 1) + c] * xc;
+            }
+            A[lane * BS_MAXR + warp] = y0;
+            A[(lane + 32) * BS_MAXR + warp] = y1;
+        }
+        __syncthreads();
+        T *X = xs + buf * BSP * BS_MAXR;
+        for (int e = tid; e < BSP * BS_MAXR; e += BSP_THREADS) {
+            const int r = e / BS_MAXR, q = e % BS_MAXR;
+            const T v = (r < rows && q < nr) ? A[e] : T(0);
+            X[e] = v;
+            if (r < rows && q < nr) P.x[(size_t)(r0 + r) * P.ldx + P.c0 + q] = v;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            bs_st_release(&P.flags[nblk - 1 - p], P.epoch);
+        }
+        if (k + 1 < n_own) prefetch_diag(k + 1);
+    };
+
+    // acc[k] -= U(block of k, block p_src) * X, X the source's solution (BSP x nr)
+    auto update = [&](int k, int p_src, const T *X) {
+        const int p = cta + k * G, r0 = r0_of(p), rows = rows_of(p);
+        const int c0 = r0_of(p_src), cols = rows_of(p_src);
+        const int r = tid >> 2, part = tid & 3;  // 16 columns per thread
+        T s[BS_MAXR];
+#pragma unroll
+        for (int q = 0; q < BS_MAXR; q++) s[q] = T(0);
+        if (r < rows) {
+            const T *u = P.a + (size_t)(r0 + r) * P.ld + c0 + part * 16;
+            T v[16];
+            if (part * 16 + 16 <= cols) {
+#pragma unroll
+                for (int e = 0; e < 16; e++) v[e] = __ldg(u + e);
+            } else {
+#pragma unroll
+                for (int e = 0; e < 16; e++) v[e] = (part * 16 + e < cols) ? __ldg(u + e) : T(0);
+            }
+#pragma unroll
+            for (int e = 0; e < 16; e++)
+#pragma unroll
+                for (int q = 0; q < BS_MAXR; q++)
+                    if (q < nr) s[q] += v[e] * X[(part * 16 + e) * BS_MAXR + q];
+        }
+#pragma unroll
+        for (int q = 0; q < BS_MAXR; q++) {
+            s[q] += __shfl_xor_sync(0xffffffffu, s[q], 1);
+            s[q] += __shfl_xor_sync(0xffffffffu, s[q], 2);
+        }
+        if (part == 0 && r < rows)
+#pragma unroll
+            for (int q = 0; q < BS_MAXR; q++)
+                if (q < nr) acc[((size_t)k * BSP + r) * BS_MAXR + q] -= s[q];
+    };
+
+    int next = 0;
+    if (n_own > 0) prefetch_diag(0);
+    if (n_own > 0 && cta == 0) {  // the bottom block needs no update
+        solve(0, 0);
+        next = 1;
+    }
+    const unsigned long long t0 = globaltimer_ns();
+    for (int p_src = 0; p_src < nblk; p_src++) {
+        const int buf = p_src & 1;
+        T *X = xs + buf * BSP * BS_MAXR;
+        if (p_src % G != cta) {
+            // wait for the source block's publication, then read its x through L2
+            if (tid == 0) {
+                const unsigned *f = &P.flags[nblk - 1 - p_src];
+                unsigned spins = 0;
+                while (bs_ld_acquire(f) != P.epoch) {
+                    if ((++spins & 255u) == 0 &&
+                        (*(volatile int *)&P.status[1] != 0 || globaltimer_ns() - t0 > WAIT_LIMIT_NS)) {
+                        if (*(volatile int *)&P.status[1] == 0) record_error(P.status, ERR_BARRIER_TIMEOUT, 6);
+                        s_fail = 1;
+                        break;
+                    }
+                }
+            }
+            __syncthreads();
+            if (s_fail) return;
+            const int r0 = r0_of(p_src), rows = rows_of(p_src);
+            for (int e = tid; e < BSP * BS_MAXR; e += BSP_THREADS) {
+                const int r = e / BS_MAXR, q = e % BS_MAXR;
+                X[e] = (r < rows && q < nr) ? __ldcg(P.x + (size_t)(r0 + r) * P.ldx + P.c0 + q) : T(0);
+            }
+            __syncthreads();
+        }
+        const int k_first = next;
+        if (k_first < n_own) {
+            update(k_first, p_src, X);
+            if (cta + k_first * G == p_src + 1) {
+                __syncthreads();
+                solve(k_first, buf ^ 1);
+                next = k_first + 1;
+            }
+        }
+        for (int k = k_first + 1; k < n_own; k++) update(k, p_src, X);
+        __syncthreads();  // X (this buffer) is overwritten two sources later
+    }
+}
+
+template <typename T>
+static cudaError_t launch_backsolve_persistent(const T *a, long ld, int n, int nrhs, T *x, long ldx,
+                                               const BsBuffers &bs, cudaStream_t st, bool *used)
+{
+    *used = false;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int nblk = (n + BSP - 1) / BSP;
+    if (nblk > bs.cap) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(backsolve_persistent_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         200 * 1024);
+    if (e != cudaSuccess) return e;
+    // two CTAs per SM where they fit: each then owns half as many blocks, so
+    // less of its work sits between a publication and the next block's solve
+    int G = 0, n_own = 0;
+    size_t smem = 0;
+    for (int want = 2; want >= 1 && G == 0; want--) {
+        const int g = nblk < want * sms ? nblk : want * sms;
+        const int own = (nblk + g - 1) / g;
+        const size_t sm = ((size_t)own * BSP * BS_MAXR + BSP * (BSP + 1) + 2 * BSP * BS_MAXR) * sizeof(T);
+        if (sm > 200 * 1024) continue;
+        int per_sm = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, backsolve_persistent_kernel<T>, BSP_THREADS, sm);
+        if (e != cudaSuccess) return e;
+        if (per_sm >= want || g == nblk) {
+            if ((long)per_sm * sms < g) continue;
+            G = g;
+            n_own = own;
+            smem = sm;
+        }
+    }
+    if (G == 0) return cudaSuccess;  // the blocked launches take it
+    (void)n_own;
+    for (int c0 = 0; c0 < nrhs; c0 += BS_MAXR) {
+        BsParams<T> P{a, ld, n, nblk, x, ldx, c0, nrhs - c0 < BS_MAXR ? nrhs - c0 : BS_MAXR, bs.flags, 0u, bs.status};
+        P.epoch = ++*bs.epoch;
+        if (P.epoch == 0) P.epoch = ++*bs.epoch;
+        void *args[] = {&P};
+        count_launch();
+        e = cudaLaunchCooperativeKernel((const void *)backsolve_persistent_kernel<T>, dim3(G), dim3(BSP_THREADS), args,
+                                        smem, st);
+        if (e != cudaSuccess) return e;
+    }
+    *used = true;
+    return cudaSuccess;
+}
+
+template <typename T>
+static cudaError_t launch_backsolve_any(const T *a, long ld, int n, int nrhs, T *x, long ldx, const BsBuffers *bs,
+                                       cudaStream_t st)
+{
+    if (bs && bs->flags && n >= BSP_PERSISTENT_MIN_N) {
+        bool used = false;
+        cudaError_t e = launch_backsolve_persistent(a, ld, n, nrhs, x, ldx, *bs, st, &used);
+        if (e != cudaSuccess || used) return e;
+    }
     return launch_backsolve_t(a, ld, n, nrhs, x, ldx, st);
 }
 
-cudaError_t launch_backsolve(const float *a, long ld, int n, int nrhs, float *x, long ldx, cudaStream_t st)
+cudaError_t launch_backsolve(const double *a, long ld, int n, int nrhs, double *x, long ldx, const BsBuffers *bs,
+                             cudaStream_t st)
 {
-    return launch_backsolve_t(a, ld, n, nrhs, x, ldx, st);
+    return launch_backsolve_any(a, ld, n, nrhs, x, ldx, bs, st);
+}
+
+cudaError_t launch_backsolve(const float *a, long ld, int n, int nrhs, float *x, long ldx, const BsBuffers *bs,
+                             cudaStream_t st)
+{
+    return launch_backsolve_any(a, ld, n, nrhs, x, ldx, bs, st);
 }
 
 // out[k] = 1 / a[k][k] (1 where the pivot is exactly zero), the same value the

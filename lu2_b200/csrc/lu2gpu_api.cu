@@ -117,9 +117,41 @@ struct lu2gpu_ctx {
     long launches[PH_COUNT] = {};
     // workspaces of the precision form (lu2gpu_mixed_solve), allocated on first use
     struct MixedWork *mx = nullptr;
+    // publication flags of the persistent back substitution (one per 64-row block)
+    unsigned *d_bsflags = nullptr;
+    int bsflags_cap = 0;
+    unsigned bs_epoch = 0;
+    BsBuffers bs{};
 };
 
 static void free_mixed(lu2gpu_ctx *c);
+
+// the back substitution's flags for an order-n system (null when they cannot
+// be had: the blocked launches then do it)
+static const BsBuffers *bs_buffers(lu2gpu_ctx *c, int n)
+{
+    if (c->fixed_scratch) return nullptr;
+    const int need = (n + 63) / 64;
+    if (need > c->bsflags_cap) {
+        cudaFree(c->d_bsflags);
+        c->d_bsflags = nullptr;
+        c->bsflags_cap = 0;
+        const int cap = need + 256;
+        if (cudaMalloc(&c->d_bsflags, (size_t)cap * sizeof(unsigned)) != cudaSuccess ||
+            cudaMemsetAsync(c->d_bsflags, 0, (size_t)cap * sizeof(unsigned), c->stream) != cudaSuccess) {
+            cudaGetLastError();
+            cudaFree(c->d_bsflags);
+            c->d_bsflags = nullptr;
+            return nullptr;
+        }
+        c->bsflags_cap = cap;
+    }
+    c->bs.flags = c->d_bsflags;
+    c->bs.cap = c->bsflags_cap;
+    c->bs.epoch = &c->bs_epoch;
+    c->bs.status = c->d_status;
+    return &c->bs;
+}
 
 struct DeviceGuard {
     int prev = -1;
@@ -233,6 +265,7 @@ extern "C" int lu2gpu_destroy(lu2gpu_ctx *c)
     if (c->ev_panel) cudaEventDestroy(c->ev_panel);
     cudaFree(c->d_ipiv);
     cudaFree(c->d_dinv);
+    cudaFree(c->d_bsflags);
     for (int i = 0; i < 4; i++) cudaFree(c->d_stage[i]);
     if (c->copy_stream) {
         cudaStreamSynchronize(c->copy_stream);
@@ -723,7 +756,7 @@ extern "C" int lu2gpu_backsolve(lu2gpu_ctx *c, int n, int nrhs, const double *a,
     if (rc) return rc;
     {
         PhaseTimer t(c, PH_BACKSOLVE);
-        K_TRY(launch_backsolve(a, lda, n, nrhs, x, ldx, c->stream));
+        K_TRY(launch_backsolve(a, lda, n, nrhs, x, ldx, bs_buffers(c, n), c->stream));
     }
     return end_status(c, "lu2gpu_backsolve");
 }
@@ -751,7 +784,7 @@ extern "C" int lu2gpu_lusolve(lu2gpu_ctx *c, int n, int nrhs, double *a, long ld
     if (rc) return rc;
     {
         PhaseTimer t(c, PH_BACKSOLVE);
-        K_TRY(launch_backsolve(a, lda, n, nrhs, a + n, lda, c->stream));
+        K_TRY(launch_backsolve(a, lda, n, nrhs, a + n, lda, bs_buffers(c, n), c->stream));
     }
     if (ipiv) CU_TRY(cudaMemcpyAsync(ipiv, c->d_ipiv, (size_t)n * sizeof(int), cudaMemcpyDeviceToDevice, c->stream));
     return end_status(c, "lu2gpu_lusolve");
@@ -788,7 +821,7 @@ extern "C" int lu2gpu_solve(lu2gpu_ctx *c, int n, const double *a, long lda, int
     }
     {
         PhaseTimer t(c, PH_BACKSOLVE);
-        K_TRY(launch_backsolve(a, lda, n, nrhs, b, ldb, c->stream));
+        K_TRY(launch_backsolve(a, lda, n, nrhs, b, ldb, bs_buffers(c, n), c->stream));
     }
     return end_status(c, "lu2gpu_solve");
 }
@@ -1336,7 +1369,7 @@ static int lumcolumn_host(int n, double *a, double *b, int m, int *pv)
                              cudaMemcpyDeviceToDevice, c->stream));
     {
         PhaseTimer t(c, PH_BACKSOLVE);
-        K_TRY(launch_backsolve(d, ld, n, 1, x, 1, c->stream));
+        K_TRY(launch_backsolve(d, ld, n, 1, x, 1, bs_buffers(c, n), c->stream));
     }
     if (pinned) {
         CU_TRY(cudaEventRecord(c->copy_ev, c->copy_stream));
@@ -1507,7 +1540,7 @@ static int backsub_host(int n, const double *a, double *b)
                              cudaMemcpyHostToDevice, c->stream));
     CU_TRY(cudaMemcpy2DAsync(x, sizeof(double), d + n, ld * sizeof(double), sizeof(double), n,
                              cudaMemcpyDeviceToDevice, c->stream));
-    K_TRY(launch_backsolve(d, ld, n, 1, x, 1, c->stream));
+    K_TRY(launch_backsolve(d, ld, n, 1, x, 1, bs_buffers(c, n), c->stream));
     CU_TRY(cudaMemcpyAsync(b, x, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     return end_status(c, "backward_sub");
 }
@@ -1769,7 +1802,7 @@ extern "C" int lu2gpu_lusolve_noalloc(int n, int nrhs, double *a, long lda, int 
     // block row are written before they are read in every call.
     if ((rc = begin_status(&c))) return rc;
     if ((rc = factor_enqueue(&c, n, nrhs, a, lda, nb, pivot_mode))) return rc;
-    K_TRY(launch_backsolve(a, lda, n, nrhs, a + n, lda, c.stream));
+    K_TRY(launch_backsolve(a, lda, n, nrhs, a + n, lda, nullptr, c.stream));
     return end_status(&c, "lu2gpu_lusolve_noalloc");
 }
 
@@ -2009,7 +2042,7 @@ static int solve32_enqueue(lu2gpu_ctx *c, int n, const float *a, long ld, int nb
         if (i + w < n)
             K_TRY(launch_gemv_sub(a + (size_t)(i + w) * ld + i, ld, n - i - w, w, v + i, v + i + w, c->stream));
     }
-    K_TRY(launch_backsolve(a, ld, n, 1, v, 1, c->stream));
+    K_TRY(launch_backsolve(a, ld, n, 1, v, 1, bs_buffers(c, n), c->stream));
     return 0;
 }
 

@@ -143,9 +143,21 @@ cudaError_t launch_transpose(const double *in, long ldi, double *out, long ldo, 
 
 // x = U'^{-1} y for the unit upper triangle of a[0..n)[0..n) (lu2's backward_sub,
 // lu2.c:110-116); y (n x nrhs, row stride ldx) is overwritten by x.  For lu2's
-// own layout x = a + n, ldx = ld.
-cudaError_t launch_backsolve(const double *a, long ld, int n, int nrhs, double *x, long ldx, cudaStream_t st);
-cudaError_t launch_backsolve(const float *a, long ld, int n, int nrhs, float *x, long ldx, cudaStream_t st);
+// own layout x = a + n, ldx = ld.  With bs (flags for n / 64 blocks, zeroed
+// once; a host epoch counter; the status words) and n >= BSP_PERSISTENT_MIN_N
+// one persistent cooperative launch per 8 right-hand sides does it; otherwise
+// blocked launches (one per 128-row block and one per update).
+struct BsBuffers {
+    unsigned *flags = nullptr;  // [cap], zeroed at allocation
+    int cap = 0;
+    unsigned *epoch = nullptr;  // host-side counter, advanced per launch
+    int *status = nullptr;
+};
+constexpr int BSP_PERSISTENT_MIN_N = 4096;
+cudaError_t launch_backsolve(const double *a, long ld, int n, int nrhs, double *x, long ldx, const BsBuffers *bs,
+                             cudaStream_t st);
+cudaError_t launch_backsolve(const float *a, long ld, int n, int nrhs, float *x, long ldx, const BsBuffers *bs,
+                             cudaStream_t st);
 
 // out[k] = 1 / a[k][k] (1 for an exactly zero pivot)
 cudaError_t launch_diag_inv(const double *a, long ld, int n, double *out, cudaStream_t st);
