@@ -240,6 +240,18 @@ int lu2gpu_bf16_update_dev(lu2gpu_ctx *ctx, int M, int N, int K, const void *a, 
 int lu2gpu_gmres_solve(lu2gpu_ctx *ctx, int n, const double *a, long lda, const double *b, double *x, int nb,
                        int update, int restart, double inner_tol, int max_iter, double *out);
 
+/* The precision forms' factorization on its own (the preconditioner of
+ * lu2gpu_mixed_solve and lu2gpu_gmres_solve; no counterpart in the
+ * reference): lu2's LU (lu2.c:1122-1144 storage: row-scaled unit U', L'
+ * below, earlier panels' L columns not swapped by later panels) of an FP32
+ * copy of the FP64 device matrix a, the panels in FP32, the top-level trailing
+ * updates with `update` operands (LU2GPU_UPDATE_BF16, nb in {64, 128, 192,
+ * 256}; LU2GPU_UPDATE_FP8, nb in {128, 256}).  f (device, n x n FP32, row
+ * stride ldf >= n) receives the factors, ipiv (device, n ints, may be NULL)
+ * the pivot sequence.  a is not modified.  Synchronous; > 0 on a zero pivot. */
+int lu2gpu_lowp_factor(lu2gpu_ctx *ctx, int n, const double *a, long lda, int nb, int update, float *f, long ldf,
+                       int *ipiv);
+
 /* The FP8 form's trailing update on its own: a (M x K) and bt (N x K) FP32
  * device matrices (row strides lda, ldb multiples of 4, 16-byte aligned) are
  * quantized to E4M3 with one power-of-two scale per 128 x 128 tile, then c

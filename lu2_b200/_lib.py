@@ -92,6 +92,7 @@ SIGNATURES = {
     "lu2gpu_test_leaf_withhold": (C.c_int, [vp, C.c_int, C.c_double]),
     "lu2gpu_swaprows_dev": (C.c_int, [vp, C.c_int, vp, C.c_long, C.c_int, C.c_int, vp, vp, C.c_int, C.c_int]),
     "lu2gpu_solve_triangle_dev": (C.c_int, [vp, C.c_int, vp, C.c_long, vp, C.c_long, C.c_int, vp]),
+    "lu2gpu_lowp_factor": (C.c_int, [vp, C.c_int, vp, C.c_long, C.c_int, C.c_int, vp, C.c_long, vp]),
 }
 
 

@@ -2672,6 +2672,41 @@ static int precond_apply(lu2gpu_ctx *c, int n, long ld32, int nb, const double *
     return 0;
 }
 
+// The precision forms' factorization on its own (what lu2gpu_mixed_solve and
+// lu2gpu_gmres_solve precondition with): lu2's LU of an FP32 copy of a, the
+// panels in FP32, the top-level trailing updates with BF16 or E4M3 operands.
+extern "C" int lu2gpu_lowp_factor(lu2gpu_ctx *c, int n, const double *a, long lda, int nb, int update,
+                                  float *f, long ldf, int *ipiv)
+{
+    if (!c || n <= 0 || !a || lda < n || !f || ldf < n) {
+        set_error("lu2gpu_lowp_factor: bad arguments");
+        return LU2GPU_ERR_ARG;
+    }
+    if ((lda & 1) || (reinterpret_cast<uintptr_t>(a) & 15)) {
+        set_error("lu2gpu_lowp_factor: A must be 16-byte aligned with an even row stride");
+        return LU2GPU_ERR_ARG;
+    }
+    if (!((update == LU2GPU_UPDATE_BF16 && nb >= 64 && nb <= 256 && nb % 64 == 0) ||
+          (update == LU2GPU_UPDATE_FP8 && (nb == 128 || nb == 256)))) {
+        set_error("lu2gpu_lowp_factor: update %d with nb=%d (BF16: 64..256 step 64; FP8: 128 or 256)", update, nb);
+        return LU2GPU_ERR_ARG;
+    }
+    DeviceGuard g(c->device);
+    const long ld32 = ((long)n + 31) & ~31L;
+    int rc = mixed_work(c, n, ld32, nb);
+    if (rc) return rc;
+    MixedWork *m = c->mx;
+    m->update = update;
+    if (update == LU2GPU_UPDATE_FP8 && (rc = fp8_work(c, n, nb))) return rc;
+    if ((rc = begin_status(c))) return rc;
+    K_TRY(launch_f64_to_f32(a, lda, m->a32, ld32, n, n, c->stream));
+    if ((rc = factor32_or_fail(c, n, m->a32, ld32, nb, LU2GPU_PIVOT_PARTIAL))) return rc;
+    CU_TRY(cudaMemcpy2DAsync(f, (size_t)ldf * sizeof(float), m->a32, (size_t)ld32 * sizeof(float),
+                             (size_t)n * sizeof(float), n, cudaMemcpyDeviceToDevice, c->stream));
+    if (ipiv) CU_TRY(cudaMemcpyAsync(ipiv, c->d_ipiv, (size_t)n * sizeof(int), cudaMemcpyDeviceToDevice, c->stream));
+    return end_status(c, "lu2gpu_lowp_factor");
+}
+
 extern "C" int lu2gpu_gmres_solve(lu2gpu_ctx *c, int n, const double *a, long lda, const double *b, double *x, int nb,
                                   int update, int restart, double inner_tol, int max_iter, double *out)
 {
@@ -2764,7 +2799,7 @@ extern "C" int lu2gpu_gmres_solve(lu2gpu_ctx *c, int n, const double *a, long ld
         if ((rc = precond_apply(c, n, ld32, nb, r, z))) return rc;
         double beta0 = 0;
         if ((rc = norm_of(z, &beta0))) return rc;
-        if (!std::isfinite(beta0)) {  // the low-precision factors overflowed
+        if (!std::isfinite(beta0)) {  // the FP32 solve with the low-precision factors overflowed
             finite = false;
             break;
         }
@@ -2849,8 +2884,8 @@ extern "C" int lu2gpu_gmres_solve(lu2gpu_ctx *c, int n, const double *a, long ld
     }
     if (rc) return rc;
     if (!finite) {
-        set_error("lu2gpu_gmres_solve: the low-precision factors are not finite (element growth in the "
-                  "factorization); no refinement possible");
+        set_error("lu2gpu_gmres_solve: applying the low-precision factors overflowed FP32 (their pivots grew "
+                  "geometrically: the low-precision updates are too coarse for this matrix); no refinement possible");
         return LU2GPU_ERR_NOCONV;
     }
     if (!(hpl < 16.0)) {

@@ -185,10 +185,16 @@ class Context:
         rc = lib().lu2gpu_gmres_solve(self._h, n, _ptr(a), lda, _ptr(b), _ptr(x), nb, update, restart, inner_tol,
                                       max_iter, _ptr(out))
         res = {"status": rc, "refinements": int(out[0]), "gmres_iterations": int(out[1]), "hpl": float(out[2]),
-               "factor_s": float(out[3]), "refine_s": float(out[4]), "finite_factors": bool(out[5])}
+               "factor_s": float(out[3]), "refine_s": float(out[4]), "finite_factors": bool(out[5])}  # finite_factors: the preconditioner's FP32 solve stayed finite
         if rc < 0 and rc != -6:
             raise Lu2GpuError("lu2gpu_gmres_solve", rc)
         return res
+
+    def lowp_factor(self, a, n: int, lda: int, nb: int, update: int, f, ldf: int, ipiv=None) -> int:
+        """The precision forms' factorization (FP32 panels, BF16 or E4M3 trailing
+        updates) of the FP64 device matrix a into the FP32 device array f."""
+        return _check("lu2gpu_lowp_factor", lib().lu2gpu_lowp_factor(self._h, n, _ptr(a), lda, nb, update, _ptr(f), ldf,
+                                                                       _ptr(ipiv)))
 
     def fp8_update(self, M, N, K, a32, lda, bt32, ldb, c32, ldc, a_deq=None, bt_deq=None) -> None:
         """c -= q(a) q(bt)^T with per-128x128-tile E4M3 quantization (FP32 device arrays)."""

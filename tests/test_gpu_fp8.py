@@ -118,3 +118,41 @@ def test_gmres_ir_rejects_bad_arguments(ctx):
         args.update(kw)
         with pytest.raises(L.Lu2GpuError):
             ctx.gmres_solve(a, n, ld, b, x, args["nb"], update=args["update"], restart=args["restart"])
+
+
+@pytest.mark.parametrize("kind,update,upd", [("general", L.UPDATE_FP8, "fp8"), ("dd", L.UPDATE_FP8, "fp8"),
+                                             ("general", L.UPDATE_BF16, "bf16")])
+def test_lowp_factors_match_the_cpu_simulation(ctx, oracle, kind, update, upd):
+    """The GPU's precision-form factors (lu2gpu_lowp_factor) against the CPU
+    simulation of the same arithmetic (tests/lowp_lu_sim.py) at n = 2048:
+    backward error ||P A - L U|| / ||A|| within a factor 2 of the
+    simulation's (the two differ only in FP32 rounding order, which moves
+    single E4M3 roundings), and the same verdict on the preconditioner: for a
+    general matrix with E4M3 updates ||I - M^-1 A|| >> 1 (the divergence the
+    FP8 form reports), for a diagonally dominant one << 1."""
+    import os
+    import sys
+
+    import torch
+
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from lowp_lu_sim import backward_error, lowp_lu, lu2_factors_to_plu, precond_rho
+
+    n, nb = 2048, 256
+    a, ld, _ = _system(ctx, n, 1, kind=1 if kind == "dd" else 0)
+    f = torch.empty((n, n), dtype=torch.float32, device="cuda")
+    ipiv = torch.zeros(n, dtype=torch.int32, device="cuda")
+    assert ctx.lowp_factor(a, n, ld, nb, update, f, n, ipiv) == 0
+    a0 = a.cpu().numpy()[:, :n]
+    lo, up, perm = lu2_factors_to_plu(f.cpu().numpy(), ipiv.cpu().numpy(), nb)
+    be_gpu = backward_error(a0, lo, up, perm)
+    rho_gpu = precond_rho(a0, lo, up, perm, iters=10)
+    slo, sup, sperm = lowp_lu(a0, nb, upd)
+    be_sim = backward_error(a0, slo, sup, sperm)
+    print("lowp %s %s n=%d: backward error gpu %.3e sim %.3e, ||I - M^-1 A|| gpu %.3g" % (upd, kind, n, be_gpu, be_sim,
+                                                                                        rho_gpu))
+    assert be_sim / 2 < be_gpu < 2 * be_sim
+    if kind == "dd":
+        assert rho_gpu < 1e-2
+    else:
+        assert rho_gpu > 10
