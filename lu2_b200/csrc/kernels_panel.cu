@@ -85,6 +85,88 @@ __device__ __forceinline__ void swap_st(T *p, int avail, const T *in)
     }
 }
 
+// The composed permutation of the exchanges k <-> ipiv[k] - goff, k = k0..k1-1
+// (see above), built by the whole CTA: slot i moves row src[i] to row dst[i];
+// slots 0..npiv-1 are the rows k0..k1-1 (in order), the others the rows >= k1
+// the exchanges name.  P and A: npiv ints each, src and dst: 2 npiv each.
+// Returns false (every thread) when the call must do nothing: an earlier wait
+// gave up, or a pivot lies outside [k, nrows) (then ERR_BAD_ARG is recorded).
+__device__ bool swap_plan(const int *__restrict__ ipiv, int goff, int k0, int k1, int nrows, int *P, int *A, int *src,
+                          int *dst, int *p_nslot, int *p_bad, int *status)
+{
+    const int npiv = k1 - k0, tid = threadIdx.x, nth = blockDim.x;
+    int &s_nslot = *p_nslot, &s_bad = *p_bad;
+    if (status && *(volatile int *)&status[1] != 0) return false;
+    if (tid == 0) {
+        s_bad = 0;
+        s_nslot = npiv;
+    }
+    __syncthreads();
+    for (int t = tid; t < npiv; t += nth) {
+        const int p = __ldg(ipiv + k0 + t) - goff;
+        P[t] = p;
+        A[t] = -1;
+        if (p < k0 + t || p >= nrows) s_bad = 1;
+    }
+    __syncthreads();
+    if (s_bad) {
+        if (blockIdx.x == 0 && tid == 0 && status) record_error(status, ERR_BAD_ARG, 3);
+        return false;
+    }
+    for (int i = tid; i < npiv; i += nth) {
+        const int q = P[i];
+        if (q != k0 + i && q < k1) atomicMax(&A[q - k0], i);
+    }
+    __syncthreads();
+    for (int t = tid; t < npiv; t += nth)
+        if (A[t] < 0) A[t] = -(k0 + t) - 1;
+    __syncthreads();
+    {
+        // pointer jumping, double-buffered through src (free until the slots
+        // are written): after r rounds every pointer has advanced 2^r links or
+        // reached its root, and a chain has fewer than npiv links
+        int *cur = A, *nxt = src;
+        for (int span = 1; span < npiv; span <<= 1) {
+            for (int t = tid; t < npiv; t += nth) {
+                const int v = cur[t];
+                nxt[t] = (v >= 0) ? cur[v] : v;
+            }
+            __syncthreads();
+            int *tmp = cur;
+            cur = nxt;
+            nxt = tmp;
+        }
+        if (cur != A) {
+            for (int t = tid; t < npiv; t += nth) A[t] = cur[t];
+            __syncthreads();
+        }
+    }
+    for (int t = tid; t < npiv; t += nth) {
+        const int p = P[t], k = k0 + t;
+        int s;
+        if (p == k) {
+            s = -A[t] - 1;
+        } else {
+            int j = t - 1;
+            while (j >= 0 && P[j] != p) j--;
+            s = (j >= 0) ? -A[j] - 1 : p;
+            if (p >= k1) {
+                int q = t + 1;
+                while (q < npiv && P[q] != p) q++;
+                if (q == npiv) {  // the last exchange that names row p
+                    const int e = atomicAdd(&s_nslot, 1);
+                    src[e] = -A[t] - 1;
+                    dst[e] = p;
+                }
+            }
+        }
+        src[t] = s;
+        dst[t] = k;
+    }
+    __syncthreads();
+    return true;
+}
+
 // NS > 0: every thread keeps its NS row segments of a chunk in registers
 // (all NS loads in flight at once, one barrier per chunk, no staging in
 // shared memory; used while the slots fit, nslot <= NS * rows per pass);
@@ -108,74 +190,7 @@ __global__ void __launch_bounds__(SWAP_THREADS, NS > 0 ? 2 : 1)
     __shared__ int s_nslot, s_bad;
     const int tid = threadIdx.x;
 
-    if (status && *(volatile int *)&status[1] != 0) return;
-    if (tid == 0) {
-        s_bad = 0;
-        s_nslot = npiv;
-    }
-    __syncthreads();
-    for (int t = tid; t < npiv; t += SWAP_THREADS) {
-        const int p = __ldg(ipiv + k0 + t) - goff;
-        P[t] = p;
-        A[t] = -1;
-        if (p < k0 + t || p >= nrows) s_bad = 1;
-    }
-    __syncthreads();
-    if (s_bad) {
-        if (blockIdx.x == 0 && tid == 0 && status) record_error(status, ERR_BAD_ARG, 3);
-        return;
-    }
-    for (int i = tid; i < npiv; i += SWAP_THREADS) {
-        const int q = P[i];
-        if (q != k0 + i && q < k1) atomicMax(&A[q - k0], i);
-    }
-    __syncthreads();
-    for (int t = tid; t < npiv; t += SWAP_THREADS)
-        if (A[t] < 0) A[t] = -(k0 + t) - 1;
-    __syncthreads();
-    {
-        // pointer jumping, double-buffered through src (free until the slots
-        // are written): after r rounds every pointer has advanced 2^r links or
-        // reached its root, and a chain has fewer than npiv links
-        int *cur = A, *nxt = src;
-        for (int span = 1; span < npiv; span <<= 1) {
-            for (int t = tid; t < npiv; t += SWAP_THREADS) {
-                const int v = cur[t];
-                nxt[t] = (v >= 0) ? cur[v] : v;
-            }
-            __syncthreads();
-            int *tmp = cur;
-            cur = nxt;
-            nxt = tmp;
-        }
-        if (cur != A) {
-            for (int t = tid; t < npiv; t += SWAP_THREADS) A[t] = cur[t];
-            __syncthreads();
-        }
-    }
-    for (int t = tid; t < npiv; t += SWAP_THREADS) {
-        const int p = P[t], k = k0 + t;
-        int s;
-        if (p == k) {
-            s = -A[t] - 1;
-        } else {
-            int j = t - 1;
-            while (j >= 0 && P[j] != p) j--;
-            s = (j >= 0) ? -A[j] - 1 : p;
-            if (p >= k1) {
-                int q = t + 1;
-                while (q < npiv && P[q] != p) q++;
-                if (q == npiv) {  // the last exchange that names row p
-                    const int e = atomicAdd(&s_nslot, 1);
-                    src[e] = -A[t] - 1;
-                    dst[e] = p;
-                }
-            }
-        }
-        src[t] = s;
-        dst[t] = k;
-    }
-    __syncthreads();
+    if (!swap_plan(ipiv, goff, k0, k1, nrows, P, A, src, dst, &s_nslot, &s_bad, status)) return;
     const int nslot = s_nslot;
     const int cq = (tid % TPR) * V, r0 = tid / TPR;
     const int nchunk = (ce - cs + COLS - 1) / COLS;
