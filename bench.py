@@ -772,6 +772,8 @@ def main() -> int:
                     help="back substitution alone: factor the order-n system, then time lu2gpu_backsolve")
     ap.add_argument("--batch-ir", action="store_true",
                     help="--profile-batched in the FP32-LU + FP64 IR mode")
+    ap.add_argument("--batch-nmin", type=int, default=16, help="--profile-batched: smallest order")
+    ap.add_argument("--batch-nmax", type=int, default=512, help="--profile-batched: largest order")
     ap.add_argument("--batch-config", default=None,
                     help="threads,panel_width,ctas_per_sm for --profile-batched (default: autotune)")
     ap.add_argument("--no-fp8", action="store_true", help="skip the FP8 + GMRES-IR measurement")
@@ -822,7 +824,7 @@ def main() -> int:
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
     if args.profile_batched:
-        n_b, r_b = L.batch_sizes(args.batch_count, 1, 16, 512, 0.1, 8)
+        n_b, r_b = L.batch_sizes(args.batch_count, 1, args.batch_nmin, args.batch_nmax, 0.1, 8)
         b = L.Batch(ctx, n_b, r_b)
         b.generate_seeds(1 + np.arange(args.batch_count))
         b.snapshot()  # the original systems, for the residuals
@@ -839,7 +841,9 @@ def main() -> int:
         t0 = time.perf_counter()
         info = b.solve()
         torch.cuda.synchronize()
+        flops = float(np.sum(2.0 / 3.0 * n_b.astype(np.float64) ** 3 + 2.0 * n_b.astype(np.float64) ** 2 * r_b))
         print(json.dumps({"profile_batched_s": time.perf_counter() - t0, "count": args.batch_count,
+                          "orders": [args.batch_nmin, args.batch_nmax], "gflop": flops / 1e9,
                           "config": cfg, "zero_pivots": int((info != 0).sum()),
                           "max_hpl_residual": float(b.residuals().max())}))
         b.close()

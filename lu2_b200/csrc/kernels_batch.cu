@@ -20,25 +20,10 @@
 
 namespace lu2gpu {
 
-__device__ __forceinline__ void batch_block_argmax(double &v, int &i, double *s_v, int *s_i)
-{
-    warp_argmax(v, i);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    if (lane == 0) {
-        s_v[warp] = v;
-        s_i[warp] = i;
-    }
-    __syncthreads();
-    v = lane < nw ? s_v[lane] : -1.0;
-    i = lane < nw ? s_i[lane] : INT_MAX;
-    warp_argmax(v, i);  // every warp reduces the same partials
-    __syncthreads();    // partials read before the next reduction writes them
-}
-
 constexpr int BATCH_LOAD_U = 4;  // global loads a thread keeps in flight when staging
 
 // whole system in shared memory: S (n x nc, stride nc)
-__device__ void batch_solve_smem(double *A, long ld, int n, int nrhs, double *S, int *info, double *s_v, int *s_i)
+__device__ void batch_solve_smem(double *A, long ld, int n, int nrhs, double *S, int *info)
 {
     const int nc = n + nrhs, T = blockDim.x, tid = threadIdx.x;
     // BATCH_LOAD_U loads in flight per thread
@@ -56,33 +41,40 @@ __device__ void batch_solve_smem(double *A, long ld, int n, int nrhs, double *S,
     __syncthreads();
     int first_zero = 0;
     for (int k = 0; k < n; k++) {
-        double v = -1.0;
-        int p = INT_MAX;
-        for (int r = k + tid; r < n; r += T) {
-            const double a = fabs(S[r * nc + k]);
-            if (a > v) {
-                v = a;
-                p = r;
+        // pivot search, row exchange and 1/pivot scaling by warp 0 alone
+        // (warp-synchronous), then one barrier; the rank-1 update by all
+        if (tid < 32) {
+            const int lane = tid;
+            double v = -1.0;
+            int p = INT_MAX;
+            for (int r = k + lane; r < n; r += 32) {
+                const double a = fabs(S[r * nc + k]);
+                if (a > v) {
+                    v = a;
+                    p = r;
+                }
+            }
+            warp_argmax(v, p);
+            if (p == INT_MAX) p = k;
+            if (p != k)
+                for (int c = lane; c < nc; c += 32) {
+                    const double t = S[k * nc + c];
+                    S[k * nc + c] = S[p * nc + c];
+                    S[p * nc + c] = t;
+                }
+            __syncwarp();
+            const double d = S[k * nc + k];
+            if (d != 0.0) {
+                const double inv = 1.0 / d;
+                for (int c = k + 1 + lane; c < nc; c += 32) S[k * nc + c] *= inv;
             }
         }
-        batch_block_argmax(v, p, s_v, s_i);
-        if (p == INT_MAX) p = k;
-        if (p != k)
-            for (int c = tid; c < nc; c += T) {
-                const double t = S[k * nc + c];
-                S[k * nc + c] = S[p * nc + c];
-                S[p * nc + c] = t;
-            }
         __syncthreads();
         const double d = S[k * nc + k];
         if (d == 0.0) {
             if (!first_zero) first_zero = k + 1;
-            __syncthreads();
             continue;
         }
-        const double inv = 1.0 / d;
-        for (int c = k + 1 + tid; c < nc; c += T) S[k * nc + c] *= inv;
-        __syncthreads();
         const int w = nc - k - 1, h = n - k - 1;
         for (int idx = tid; idx < h * w; idx += T) {
             const int r = k + 1 + idx / w, c = k + 1 + idx % w;
@@ -116,11 +108,11 @@ __device__ __forceinline__ void batch_dmma(double (&c)[4], double a0, double a1,
 
 // blocked LU in global memory (L2-resident), panel of pw columns in shared memory
 __device__ void batch_solve_blocked(double *A, long ld, int n, int nrhs, int pw, double *P, double *U, int *piv,
-                                    double *dinv, int *info, double *s_v, int *s_i)
+                                    double *dinv, int *info)
 {
     const int nc = n + nrhs, T = blockDim.x, tid = threadIdx.x;
-    // panel row stride: the 8 rows a warp's MMA fragment load touches fall
-    // into different banks (2 * (pw + 4) doubles = 8 banks apart for pw % 16 == 0)
+    // panel row stride pw + 1 (odd): the lanes of the panel factorization, one
+    // row each, fall into different banks
     const int ps = pw + BATCH_PANEL_PAD;
     int first_zero = 0;
     for (int k0 = 0; k0 < n; k0 += pw) {
@@ -140,44 +132,50 @@ __device__ void batch_solve_blocked(double *A, long ld, int n, int nrhs, int pw,
             }
         }
         __syncthreads();
-        for (int c = 0; c < w; c++) {
-            double v = -1.0;
-            int p = INT_MAX;
-            for (int r = c + tid; r < rows; r += T) {
-                const double a = fabs(P[r * ps + c]);
-                if (a > v) {
-                    v = a;
-                    p = r;
+        // the panel factored by warp 0 alone, warp-synchronously: one lane per
+        // row (rows lane, lane+32, ...), no CTA barrier per column; per element
+        // the same operations as a CTA-wide elimination
+        if (tid < 32) {
+            const int lane = tid;
+            for (int c = 0; c < w; c++) {
+                double v = -1.0;
+                int p = INT_MAX;
+                for (int r = c + lane; r < rows; r += 32) {
+                    const double a = fabs(P[r * ps + c]);
+                    if (a > v) {
+                        v = a;
+                        p = r;
+                    }
                 }
+                warp_argmax(v, p);
+                if (p == INT_MAX) p = c;
+                if (lane == 0) piv[c] = p;
+                if (p != c)
+                    for (int j = lane; j < w; j += 32) {
+                        const double t = P[c * ps + j];
+                        P[c * ps + j] = P[p * ps + j];
+                        P[p * ps + j] = t;
+                    }
+                __syncwarp();
+                const double d = P[c * ps + c];
+                const bool zero = (d == 0.0);
+                if (zero && !first_zero) first_zero = k0 + c + 1;
+                const double inv = zero ? 1.0 : 1.0 / d;
+                if (lane == 0) dinv[c] = inv;
+                __syncwarp();  // every lane has read the pivot before it is scaled
+                if (!zero)
+                    for (int j = lane; j < w; j += 32)
+                        if (j != c) P[c * ps + j] *= inv;
+                __syncwarp();
+                if (!zero)
+                    for (int r = c + 1 + lane; r < rows; r += 32) {
+                        const double l = P[r * ps + c];
+                        for (int j = c + 1; j < w; j++) P[r * ps + j] -= l * P[c * ps + j];
+                    }
+                __syncwarp();
             }
-            batch_block_argmax(v, p, s_v, s_i);
-            if (p == INT_MAX) p = c;
-            if (tid == 0) piv[c] = p;
-            if (p != c)
-                for (int j = tid; j < w; j += T) {
-                    const double t = P[c * ps + j];
-                    P[c * ps + j] = P[p * ps + j];
-                    P[p * ps + j] = t;
-                }
-            __syncthreads();
-            const double d = P[c * ps + c];
-            const bool zero = (d == 0.0);
-            if (zero && !first_zero) first_zero = k0 + c + 1;
-            const double inv = zero ? 1.0 : 1.0 / d;
-            if (tid == 0) dinv[c] = inv;
-            if (!zero)
-                for (int j = tid; j < w; j += T)
-                    if (j != c) P[c * ps + j] *= inv;
-            __syncthreads();
-            if (!zero) {
-                const int wj = w - c - 1, hr = rows - c - 1;
-                for (int idx = tid; idx < hr * wj; idx += T) {
-                    const int r = c + 1 + idx / wj, j = c + 1 + idx % wj;
-                    P[r * ps + j] -= P[r * ps + c] * P[c * ps + j];
-                }
-            }
-            __syncthreads();
         }
+        __syncthreads();  // (first_zero is tracked by warp 0, whose thread 0 reports it)
         for (int idx = tid; idx < rows * w; idx += T) {
             const int r = idx / w, c = idx - r * w;
             A[(size_t)(k0 + r) * ld + k0 + c] = P[r * ps + c];
@@ -333,8 +331,6 @@ __global__ void __launch_bounds__(512, 2) batch_lu_kernel(double *data, const Ba
                                 int *info, int pw, long smem_doubles)
 {
     extern __shared__ double bsm[];
-    __shared__ double s_v[32];
-    __shared__ int s_i[32];
     __shared__ int s_next;
     __shared__ int s_piv[64];
     __shared__ double s_dinv[64];
@@ -348,12 +344,11 @@ __global__ void __launch_bounds__(512, 2) batch_lu_kernel(double *data, const Ba
         const BatchSys S = sys[i];
         double *A = data + S.off;
         if ((long)S.n * (S.n + S.nrhs) <= smem_doubles) {
-            batch_solve_smem(A, S.ld, S.n, S.nrhs, bsm, info + i, s_v, s_i);
+            batch_solve_smem(A, S.ld, S.n, S.nrhs, bsm, info + i);
         } else {
             // panel (n x pw) then the U chunk (pw x 64)
             batch_solve_blocked(A, S.ld, S.n, S.nrhs, pw, bsm, bsm + (size_t)S.n * (pw + BATCH_PANEL_PAD), s_piv, s_dinv,
-                                info + i, s_v,
-                                s_i);
+                                info + i);
         }
         __syncthreads();
     }

@@ -218,8 +218,7 @@ __global__ void __launch_bounds__(SWAP_THREADS, NS > 0 ? 2 : 1)
                 }
             }
         }
-        return;
-    }
+    } else {
     for (int chunk = blockIdx.x; chunk < nchunk; chunk += gridDim.x) {
         const int j = cs + chunk * COLS + cq;
         const int avail = ce - j;
@@ -255,6 +254,7 @@ __global__ void __launch_bounds__(SWAP_THREADS, NS > 0 ? 2 : 1)
             }
         }
         __syncthreads();
+    }
     }
 }
 

@@ -204,8 +204,9 @@ struct BatchSys {
 };
 // dynamic shared memory a CTA of the batched launch may use
 constexpr size_t BATCH_SMEM_MAX = 220 * 1024;
-// blocked path: panel row stride pw + BATCH_PANEL_PAD, U-chunk row stride (64 columns + pad)
-constexpr int BATCH_PANEL_PAD = 4;
+// blocked path: panel row stride pw + BATCH_PANEL_PAD (odd, so that lanes on
+// consecutive rows hit different banks), U-chunk row stride (64 columns + pad)
+constexpr int BATCH_PANEL_PAD = 1;
 constexpr int BATCH_U_STRIDE = 68;
 // shared-memory doubles a CTA needs for the systems sys[0..count) with panel width pw
 long batch_smem_doubles(const BatchSys *sys, int count, int pw);
