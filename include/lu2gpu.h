@@ -295,9 +295,17 @@ int lu2gpu_batch_iterations(lu2gpu_batch *b, int *iters_host);
 /* Launch shape: threads per CTA (64..512, a multiple of 32), panel width of
  * the blocked path (16..64), CTAs per SM. */
 int lu2gpu_batch_set_config(lu2gpu_batch *b, int threads, int pw, int ctas_per_sm);
-/* Time the launch shapes on this batch and keep the fastest; params_out (4
- * ints, may be NULL) = {threads, panel width, CTAs per SM, microseconds}. */
+/* Time the launch shapes on this batch (the median of three launches per
+ * candidate) and keep the fastest; in the FP64 mode then the panel width of
+ * each size bucket (n in [1,64), [64,128), [128,256), [256,...)) the same way.
+ * params_out (4 ints, may be NULL) = {threads, panel width, CTAs per SM,
+ * microseconds}.  lu2gpu_batch_set_config and lu2gpu_batch_set_mode reset the
+ * bucket widths.  No counterpart in lu2, whose block size is a fixed
+ * command-line value (lu2.c:1220-1240). */
 int lu2gpu_batch_autotune(lu2gpu_batch *b, int *params_out);
+/* The autotuned panel width per size bucket: out[2k] = the smallest n of
+ * bucket k, out[2k+1] = its width (0: the launch's); 8 ints. */
+int lu2gpu_batch_bucket_pw(lu2gpu_batch *b, int *out);
 /* Factor and solve all systems in place; info_host (count ints, may be NULL)
  * receives each system's zero-pivot status (0 or column + 1). */
 int lu2gpu_batch_solve(lu2gpu_batch *b, int *info_host);

@@ -71,6 +71,7 @@ SIGNATURES = {
     "lu2gpu_batch_set_mode": (C.c_int, [vp, C.c_int, C.c_int]),
     "lu2gpu_batch_iterations": (C.c_int, [vp, vp]),
     "lu2gpu_batch_autotune": (C.c_int, [vp, vp]),
+    "lu2gpu_batch_bucket_pw": (C.c_int, [vp, vp]),
     "lu2gpu_batch_solve": (C.c_int, [vp, vp]),
     "lu2gpu_batch_residuals": (C.c_int, [vp, vp]),
     "lu2gpu_batch_sizes": (C.c_int, [C.c_int, C.c_long, C.c_int, C.c_int, C.c_double, C.c_int, vp, vp]),

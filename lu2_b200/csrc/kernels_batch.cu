@@ -346,9 +346,11 @@ __global__ void __launch_bounds__(512, 2) batch_lu_kernel(double *data, const Ba
         if ((long)S.n * (S.n + S.nrhs) <= smem_doubles) {
             batch_solve_smem(A, S.ld, S.n, S.nrhs, bsm, info + i);
         } else {
-            // panel (n x pw) then the U chunk (pw x 64)
-            batch_solve_blocked(A, S.ld, S.n, S.nrhs, pw, bsm, bsm + (size_t)S.n * (pw + BATCH_PANEL_PAD), s_piv, s_dinv,
-                                info + i);
+            // panel (n x pw) then the U chunk (pw x 64); the system's own panel
+            // width when its size bucket has one
+            const int pwi = S.pw ? S.pw : pw;
+            batch_solve_blocked(A, S.ld, S.n, S.nrhs, pwi, bsm, bsm + (size_t)S.n * (pwi + BATCH_PANEL_PAD), s_piv,
+                                s_dinv, info + i);
         }
         __syncthreads();
     }
@@ -361,9 +363,10 @@ long batch_smem_doubles(const BatchSys *sys, int count, int pw)
     // then a 32 x 33 diagonal block; the in-shared-memory path uses whatever
     // this leaves
     long need = 0;
-    const long tail = pw * BATCH_U_STRIDE > 32 * 33 ? pw * BATCH_U_STRIDE : 32 * 33;
-    const long ps = pw + BATCH_PANEL_PAD;
     for (int i = 0; i < count; i++) {
+        const long pwi = sys[i].pw ? sys[i].pw : pw;
+        const long tail = pwi * BATCH_U_STRIDE > 32 * 33 ? pwi * BATCH_U_STRIDE : 32 * 33;
+        const long ps = pwi + BATCH_PANEL_PAD;
         const long w = sys[i].nrhs > ps ? sys[i].nrhs : ps;
         const long ni = (long)sys[i].n * w + tail;
         if (ni > need) need = ni;

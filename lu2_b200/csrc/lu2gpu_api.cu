@@ -2068,6 +2068,8 @@ extern "C" int lu2gpu_bf16_update_dev(lu2gpu_ctx *c, int M, int N, int K, const 
 // Batching form: many independent systems of uneven order in one persistent
 // launch (kernels_batch.cu), replayed from a CUDA graph.
 
+constexpr int BATCH_BUCKETS = 4;
+
 struct lu2gpu_batch {
     lu2gpu_ctx *ctx = nullptr;
     int count = 0, max_n = 0;
@@ -2088,7 +2090,10 @@ struct lu2gpu_batch {
     cudaStream_t capture = nullptr;  // private stream the graph is captured on
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    int bucket_pw[BATCH_BUCKETS] = {0, 0, 0, 0};  // autotuned panel width per size bucket (0: the launch's)
 };
+
+static int batch_clear_bucket_pw(lu2gpu_batch *b);
 
 static void batch_drop_graph(lu2gpu_batch *b)
 {
@@ -2356,7 +2361,9 @@ extern "C" int lu2gpu_batch_set_mode(lu2gpu_batch *b, int mode, int max_iter)
     const int old = b->mode;
     b->mode = mode;
     b->max_iter = max_iter;
-    int rc = batch_configure(b, 256, 32, 1);
+    int rc = batch_clear_bucket_pw(b);
+    if (rc) return rc;
+    rc = batch_configure(b, 256, 32, 1);
     if (rc) rc = batch_configure(b, 256, 16, 1);
     if (rc) b->mode = old;
     return rc;
@@ -2381,7 +2388,8 @@ extern "C" int lu2gpu_batch_set_config(lu2gpu_batch *b, int threads, int pw, int
         return LU2GPU_ERR_ARG;
     }
     DeviceGuard g(b->ctx->device);
-    return batch_configure(b, threads, pw, ctas_per_sm);
+    int rc = batch_clear_bucket_pw(b);  // one panel width for every system
+    return rc ? rc : batch_configure(b, threads, pw, ctas_per_sm);
 }
 
 // Factor and solve every system in place; the launch is captured into a CUDA
@@ -2412,15 +2420,67 @@ extern "C" int lu2gpu_batch_solve(lu2gpu_batch *b, int *info_host)
     return 0;
 }
 
+// Size buckets of the autotuner's per-bucket panel width: n in [lo_k, lo_{k+1}).
+static const int BATCH_BUCKET_LO[BATCH_BUCKETS + 1] = {1, 64, 128, 256, 1 << 30};
+
+// Panel width pw (0: the launch's) for the blocked path of every system in
+// bucket k; re-uploads the system table.
+static int batch_set_bucket_pw(lu2gpu_batch *b, int k, int pw)
+{
+    bool changed = false;
+    for (auto &S : b->sys)
+        if (S.n >= BATCH_BUCKET_LO[k] && S.n < BATCH_BUCKET_LO[k + 1] && S.pw != pw) {
+            S.pw = pw;
+            changed = true;
+        }
+    b->bucket_pw[k] = pw;
+    if (!changed) return 0;
+    batch_drop_graph(b);
+    CU_TRY(cudaMemcpy(b->d_sys, b->sys.data(), sizeof(BatchSys) * b->count, cudaMemcpyHostToDevice));
+    return 0;
+}
+
+static int batch_clear_bucket_pw(lu2gpu_batch *b)
+{
+    for (int k = 0; k < BATCH_BUCKETS; k++) {
+        int rc = batch_set_bucket_pw(b, k, 0);
+        if (rc) return rc;
+    }
+    return 0;
+}
+
+// Median of three timed launches of the current configuration, each on the
+// batch restored from its snapshot; *ms = 1e30 if a launch failed.
+static int batch_time3(lu2gpu_batch *b, cudaStream_t st, cudaEvent_t e0, cudaEvent_t e1, float *ms)
+{
+    float t[3];
+    for (int r = 0; r < 3; r++) {
+        int rc = lu2gpu_batch_restore(b);
+        if (rc) return rc;
+        CU_TRY(cudaEventRecord(e0, st));
+        if ((rc = batch_enqueue(b, st))) return rc;
+        CU_TRY(cudaEventRecord(e1, st));
+        CU_TRY(cudaEventSynchronize(e1));
+        t[r] = 0.f;
+        cudaEventElapsedTime(&t[r], e0, e1);
+    }
+    std::sort(t, t + 3);
+    *ms = t[1];
+    return 0;
+}
+
 // Time the persistent launch over launch shapes (threads per CTA, panel width,
 // CTAs per SM) on this batch's own data (restored from a snapshot before every
-// trial) and keep the fastest; params_out = {threads, pw, ctas_per_sm, best us}.
+// trial; the median of three trials per candidate) and keep the fastest; then,
+// in the FP64 mode, choose the panel width of each size bucket the same way
+// with the shape fixed.  params_out = {threads, pw, ctas_per_sm, best us}.
 extern "C" int lu2gpu_batch_autotune(lu2gpu_batch *b, int *params_out)
 {
     if (!b) return LU2GPU_ERR_ARG;
     DeviceGuard g(b->ctx->device);
     int rc = lu2gpu_batch_snapshot(b);
     if (rc) return rc;
+    if ((rc = batch_clear_bucket_pw(b))) return rc;
     cudaStream_t st = b->ctx->stream;
     const int cand_threads[3] = {128, 256, 512}, cand_pw[3] = {16, 32, 64}, cand_ctas[2] = {1, 2};
     float best = 1e30f;
@@ -2428,17 +2488,12 @@ extern "C" int lu2gpu_batch_autotune(lu2gpu_batch *b, int *params_out)
     cudaEvent_t e0, e1;
     CU_TRY(cudaEventCreate(&e0));
     CU_TRY(cudaEventCreate(&e1));
-    for (int ti = 0; ti < 3; ti++)
-        for (int pi = 0; pi < 3; pi++)
-            for (int ci = 0; ci < 2; ci++) {
+    for (int ti = 0; ti < 3 && !rc; ti++)
+        for (int pi = 0; pi < 3 && !rc; pi++)
+            for (int ci = 0; ci < 2 && !rc; ci++) {
                 if (batch_configure(b, cand_threads[ti], cand_pw[pi], cand_ctas[ci])) continue;  // does not fit
-                if ((rc = lu2gpu_batch_restore(b))) return rc;
-                CU_TRY(cudaEventRecord(e0, st));
-                if ((rc = batch_enqueue(b, st))) return rc;
-                CU_TRY(cudaEventRecord(e1, st));
-                CU_TRY(cudaEventSynchronize(e1));
-                float ms = 0;
-                cudaEventElapsedTime(&ms, e0, e1);
+                float ms = 0.f;
+                if ((rc = batch_time3(b, st, e0, e1, &ms))) break;
                 if (ms < best) {
                     best = ms;
                     bt = b->threads;
@@ -2446,9 +2501,32 @@ extern "C" int lu2gpu_batch_autotune(lu2gpu_batch *b, int *params_out)
                     bc = b->ctas_per_sm;
                 }
             }
+    if (!rc) rc = batch_configure(b, bt, bp, bc);
+    if (!rc && b->mode == LU2GPU_BATCH_FP64) {
+        // per size bucket (largest first), the launch's panel width or another
+        for (int k = BATCH_BUCKETS - 1; k >= 0 && !rc; k--) {
+            bool any = false;
+            for (const auto &S : b->sys) any |= (S.n >= BATCH_BUCKET_LO[k] && S.n < BATCH_BUCKET_LO[k + 1]);
+            if (!any) continue;
+            int keep = 0;
+            for (int pi = 0; pi < 3 && !rc; pi++) {
+                if (cand_pw[pi] == bp) continue;  // the launch's width is the time already measured
+                if ((rc = batch_set_bucket_pw(b, k, cand_pw[pi]))) break;
+                if (batch_configure(b, bt, bp, bc)) continue;  // does not fit
+                float ms = 0.f;
+                if ((rc = batch_time3(b, st, e0, e1, &ms))) break;
+                if (ms < best) {
+                    best = ms;
+                    keep = cand_pw[pi];
+                }
+            }
+            if (!rc) rc = batch_set_bucket_pw(b, k, keep);
+            if (!rc) rc = batch_configure(b, bt, bp, bc);
+        }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    if ((rc = batch_configure(b, bt, bp, bc))) return rc;
+    if (rc) return rc;
     if ((rc = lu2gpu_batch_restore(b))) return rc;
     CU_TRY(cudaStreamSynchronize(st));
     if (params_out) {
@@ -2456,6 +2534,21 @@ extern "C" int lu2gpu_batch_autotune(lu2gpu_batch *b, int *params_out)
         params_out[1] = bp;
         params_out[2] = bc;
         params_out[3] = (int)(best * 1000.f);
+    }
+    return 0;
+}
+
+// The panel width the autotuner chose for each size bucket: out[2k] = the
+// smallest n of bucket k, out[2k+1] = its panel width (0: the launch's).
+extern "C" int lu2gpu_batch_bucket_pw(lu2gpu_batch *b, int *out)
+{
+    if (!b || !out) {
+        set_error("lu2gpu_batch_bucket_pw: bad arguments");
+        return LU2GPU_ERR_ARG;
+    }
+    for (int k = 0; k < BATCH_BUCKETS; k++) {
+        out[2 * k] = BATCH_BUCKET_LO[k];
+        out[2 * k + 1] = b->bucket_pw[k];
     }
     return 0;
 }

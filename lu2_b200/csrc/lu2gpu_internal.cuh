@@ -197,10 +197,11 @@ cudaError_t launch_add_f32_to_f64(const float *d, double *x, int n, cudaStream_t
 // batching form (kernels_batch.cu)
 
 // one system of a batch: its augmented matrix (n x (n+nrhs), row stride ld)
-// starts at data + off
+// starts at data + off; pw = the panel width of its blocked path (0: the
+// launch's), set per size bucket by the autotuner
 struct BatchSys {
     long long off;
-    int n, nrhs, ld, pad_;
+    int n, nrhs, ld, pw;
 };
 // dynamic shared memory a CTA of the batched launch may use
 constexpr size_t BATCH_SMEM_MAX = 220 * 1024;

@@ -335,7 +335,14 @@ class Batch:
     def autotune(self) -> dict:
         out = np.zeros(4, dtype=np.int32)
         _check("lu2gpu_batch_autotune", lib().lu2gpu_batch_autotune(self._h, _ptr(out)))
-        return {"threads": int(out[0]), "pw": int(out[1]), "ctas_per_sm": int(out[2]), "us": int(out[3])}
+        return {"threads": int(out[0]), "pw": int(out[1]), "ctas_per_sm": int(out[2]), "us": int(out[3]),
+                "bucket_pw": self.bucket_pw()}
+
+    def bucket_pw(self) -> dict:
+        """Autotuned panel width per size bucket {smallest n: width}, width 0 = the launch's."""
+        out = np.zeros(8, dtype=np.int32)
+        _check("lu2gpu_batch_bucket_pw", lib().lu2gpu_batch_bucket_pw(self._h, _ptr(out)))
+        return {int(out[2 * k]): int(out[2 * k + 1]) for k in range(4)}
 
     def solve(self) -> np.ndarray:
         info = np.zeros(self.count, dtype=np.int32)

@@ -87,6 +87,17 @@ def test_batch_launch_shapes(ctx, small_batch, threads, pw, ctas):
     assert (small_batch.residuals() < 16).all()
 
 
+def test_batch_bucket_widths_reset_by_set_config(ctx, small_batch):
+    """A per-bucket panel width from the autotuner is dropped by set_config
+    (one width for every system again); the solve stays correct."""
+    small_batch.autotune()
+    small_batch.set_config(256, 16, 2)
+    assert all(w == 0 for w in small_batch.bucket_pw().values())
+    small_batch.restore()
+    assert (small_batch.solve() == 0).all()
+    assert (small_batch.residuals() < 16).all()
+
+
 def test_batch_panel_too_wide_is_rejected(ctx, small_batch):
     """n = 510 with a 64-column panel needs more than 220 KB of shared memory."""
     with pytest.raises(L.Lu2GpuError):
@@ -110,6 +121,8 @@ def test_batch_wide_panel_blocked_path(ctx):
 def test_batch_autotune_then_graph_replay(ctx, small_batch):
     cfg = small_batch.autotune()
     assert cfg["threads"] in (128, 256, 512) and cfg["pw"] in (16, 32, 64)
+    assert sorted(cfg["bucket_pw"]) == [1, 64, 128, 256]
+    assert all(w in (0, 16, 32, 64) for w in cfg["bucket_pw"].values())
     for _ in range(2):  # second call replays the captured graph
         small_batch.restore()
         assert (small_batch.solve() == 0).all()
