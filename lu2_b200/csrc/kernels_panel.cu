@@ -424,20 +424,21 @@ __global__ void __launch_bounds__(256) trsm_unit_lower_kernel(const E *T, long l
 // tensor pipe -- the blocked substitution of lu2's solve_triangle
 // (lu2.c:485-521).  Each warp owns 8 columns of X and keeps all K rows of them
 // in registers as MMA accumulators, so no step waits for another warp; T's
-// 16-column block b (rows below the diagonal block) is staged in shared
-// memory per step, double-buffered with cp.async, and shared by the CTA's
-// warps.  Two 4-warp CTAs share an SM, so one CTA's substitutions overlap the
+// 16-column block b (rows 16b..K-1: the diagonal block, then the rows below
+// it) is staged in shared memory per step, double-buffered with cp.async, and
+// shared by the CTA's warps.  Two 4-warp CTAs share an SM, so one CTA's substitutions overlap the
 // other's products.  Outputs: X in place (16-byte stores) and
 // bt[j*K + r] = -X[r][j] written in 128-byte column segments through a
 // per-warp scratch tile.
 constexpr int TD_WARPS = 4;
 constexpr int TD_COLS = 8 * TD_WARPS;  // columns of X per CTA
 constexpr int TD_MAXB = 16;            // K <= 256
-constexpr int TD_TP = 18;              // padded pitch (doubles): fragment rows g, g+4 in opposite bank halves
-constexpr int TD_SP = 9;               // pitch of the per-warp 16 x 8 scratch tile
-constexpr int TD_TROWS = 16 * TD_MAXB - 16;  // rows of a staged T block (below the diagonal block)
-constexpr size_t TD_SMEM =
-    (size_t)(2 * TD_TROWS * TD_TP + TD_MAXB * 16 * TD_TP + TD_WARPS * 16 * TD_SP) * sizeof(double);
+// padded pitch (doubles) of a staged T block: a half-warp's A-fragment loads
+// (rows g = 0..3, columns t = 0..3) fall on 16 distinct bank pairs (4g + t)
+constexpr int TD_TP = 20;
+constexpr int TD_SP = 9;                // pitch of the per-warp 16 x 8 scratch tile
+constexpr int TD_TROWS = 16 * TD_MAXB;  // rows of a staged T block (its diagonal block first)
+constexpr size_t TD_SMEM = (size_t)(2 * TD_TROWS * TD_TP + TD_WARPS * 16 * TD_SP) * sizeof(double);
 
 __device__ __forceinline__ void td_mma(double (&c)[4], double a0, double a1, double a2, double a3, double b0, double b1)
 {
@@ -459,30 +460,26 @@ __global__ void __launch_bounds__(TD_WARPS * 32, 2)
     trsm_dmma_kernel(const double *__restrict__ T, long ldt, double *X, long ldx, int K, int ncols, double *bt)
 {
     extern __shared__ __align__(16) double td_smem[];
-    double *Tb = td_smem;                  // [2][TD_TROWS][TD_TP]
-    double *Lv = Tb + 2 * TD_TROWS * TD_TP;  // [TD_MAXB][16][TD_TP]: the diagonal blocks, strict lower part
+    double *Tb = td_smem;  // [2][TD_TROWS][TD_TP]
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int g = lane >> 2, t = lane & 3;
-    double *S = Lv + TD_MAXB * 16 * TD_TP + warp * 16 * TD_SP;  // this warp's 16 x 8 tile
+    double *S = Tb + 2 * TD_TROWS * TD_TP + warp * 16 * TD_SP;  // this warp's 16 x 8 tile
     const int nbk = K >> 4;
     const int c0 = blockIdx.x * TD_COLS + warp * 8;
 
-    // T's column block b, rows 16(b+1)..K-1, into Tb[b & 1] (row r of the
-    // block at row r - 16(b+1)); 16-byte copies, 8 per row
+    // T's column block b, rows 16b..K-1, into Tb[b & 1] (row r of the block
+    // at row r - 16b: the diagonal block, of which the substitution reads the
+    // strict lower part, then the blocks below); 16-byte copies, 8 per row
     auto stage = [&](int b) {
         double *dst = Tb + (b & 1) * TD_TROWS * TD_TP;
-        const int rows = K - 16 * (b + 1);
+        const int rows = K - 16 * b;
         for (int q = tid; q < rows * 8; q += TD_WARPS * 32) {
             const int r = q >> 3, ch = q & 7;
-            td_cp16(dst + r * TD_TP + 2 * ch, T + (size_t)(16 * (b + 1) + r) * ldt + 16 * b + 2 * ch);
+            td_cp16(dst + r * TD_TP + 2 * ch, T + (size_t)(16 * b + r) * ldt + 16 * b + 2 * ch);
         }
         asm volatile("cp.async.commit_group;" ::: "memory");
     };
     stage(0);
-    for (int q = tid; q < nbk * 256; q += TD_WARPS * 32) {
-        const int b = q >> 8, r = (q >> 4) & 15, c = q & 15;
-        Lv[(b * 16 + r) * TD_TP + c] = (c < r) ? T[(size_t)(16 * b + r) * ldt + 16 * b + c] : 0.0;
-    }
 
     // this warp's columns of X as accumulators: block i, rows 16i+g and
     // 16i+g+8, columns c0+2t and c0+2t+1
@@ -516,7 +513,7 @@ __global__ void __launch_bounds__(TD_WARPS * 32, 2)
     for (int b = 0; b < TD_MAXB; b++) {
         if (b >= nbk) break;
         asm volatile("cp.async.wait_group 0;" ::: "memory");
-        __syncthreads();  // Tb[b & 1] (and at b = 0 the diagonal blocks) visible; step b-1's readers of Tb[(b+1) & 1] done
+        __syncthreads();  // Tb[b & 1] visible; step b-1's readers of Tb[(b+1) & 1] done
         if (b + 1 < nbk) stage(b + 1);
         // block b by forward substitution, one lane per column, through the scratch tile
         S[g * TD_SP + 2 * t] = acc[b][0];
@@ -524,8 +521,9 @@ __global__ void __launch_bounds__(TD_WARPS * 32, 2)
         S[(g + 8) * TD_SP + 2 * t] = acc[b][2];
         S[(g + 8) * TD_SP + 2 * t + 1] = acc[b][3];
         __syncwarp();
+        const double *Tc = Tb + (b & 1) * TD_TROWS * TD_TP;
         if (lane < 8) {
-            const double *Lb = Lv + b * 16 * TD_TP;
+            const double *Lb = Tc;
             double xd[16];
 #pragma unroll
             for (int r = 0; r < 16; r++) xd[r] = S[r * TD_SP + lane];
@@ -566,12 +564,11 @@ __global__ void __launch_bounds__(TD_WARPS * 32, 2)
             bb[kk][1] = S[(8 * kk + t + 4) * TD_SP + g];
         }
         __syncwarp();  // the scratch is rewritten at the next step
-        const double *Tc = Tb + (b & 1) * TD_TROWS * TD_TP;
 #pragma unroll
         for (int i = 0; i < TD_MAXB; i++) {
             if (i <= b || i >= nbk) continue;
             // s = T_ib X_b from zero, then X_i -= s: the CUDA-core solve's rounding structure
-            const double *A = Tc + (16 * (i - b - 1)) * TD_TP;
+            const double *A = Tc + (16 * (i - b)) * TD_TP;
             double sum[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
             for (int kk = 0; kk < 2; kk++)
