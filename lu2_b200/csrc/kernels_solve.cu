@@ -156,12 +156,16 @@ static cudaError_t launch_backsolve_t(const T *a, long ld, int n, int nrhs, T *x
 // order, so every element receives its updates in a fixed order; the CTA
 // owning block p+1 does that block first and solves it at once (column
 // oriented, one warp per right-hand side), so the critical path per block is
-// one 64x64 product and one 64x64 solve.  Each block of U is read once.
+// one 64x64 product and one 64x64 solve.  Each block of U is read once: a
+// CTA issues the loads of the U tiles its next BSP_AHEAD pending blocks take
+// from a source before it waits for that source's flag, so that their DRAM
+// latency overlaps the wait (the tiles do not depend on x).
 // Publication: the block's x rows, then a fence and a release store of the
 // call's epoch into the block's flag; readers acquire the flag (bounded wait)
 // and read x through L2.
 constexpr int BSP = 64;          // rows per block
 constexpr int BSP_THREADS = 256;
+constexpr int BSP_AHEAD = 2;     // U tiles per CTA loaded before a source's flag is awaited
 
 template <typename T>
 struct BsParams {
@@ -189,7 +193,7 @@ __device__ __forceinline__ void bs_st_release(unsigned *p, unsigned v)
 }
 
 template <typename T>
-__global__ void __launch_bounds__(BSP_THREADS) backsolve_persistent_kernel(BsParams<T> P)
+__global__ void __launch_bounds__(BSP_THREADS, 2) backsolve_persistent_kernel(BsParams<T> P)
 {
     extern __shared__ __align__(16) unsigned char bsp_smem[];
     const int G = gridDim.x, cta = blockIdx.x, tid = threadIdx.x;
@@ -268,17 +272,14 @@ __global__ void __launch_bounds__(BSP_THREADS) backsolve_persistent_kernel(BsPar
         if (k + 1 < n_own) prefetch_diag(k + 1);
     };
 
-    // acc[k] -= U(block of k, block p_src) * X, X the source's solution (BSP x nr)
-    auto update = [&](int k, int p_src, const T *X) {
+    // thread (r, part) of owned block k's U tile for source p_src: row r,
+    // columns 16 part .. 16 part + 15 (zero outside the tile)
+    auto load_u = [&](int k, int p_src, T (&v)[16]) {
         const int p = cta + k * G, r0 = r0_of(p), rows = rows_of(p);
         const int c0 = r0_of(p_src), cols = rows_of(p_src);
-        const int r = tid >> 2, part = tid & 3;  // 16 columns per thread
-        T s[BS_MAXR];
-#pragma unroll
-        for (int q = 0; q < BS_MAXR; q++) s[q] = T(0);
+        const int r = tid >> 2, part = tid & 3;
         if (r < rows) {
             const T *u = P.a + (size_t)(r0 + r) * P.ld + c0 + part * 16;
-            T v[16];
             if (part * 16 + 16 <= cols) {
 #pragma unroll
                 for (int e = 0; e < 16; e++) v[e] = __ldg(u + e);
@@ -286,6 +287,20 @@ __global__ void __launch_bounds__(BSP_THREADS) backsolve_persistent_kernel(BsPar
 #pragma unroll
                 for (int e = 0; e < 16; e++) v[e] = (part * 16 + e < cols) ? __ldg(u + e) : T(0);
             }
+        } else {
+#pragma unroll
+            for (int e = 0; e < 16; e++) v[e] = T(0);
+        }
+    };
+
+    // acc[k] -= U(block of k, block p_src) * X, X the source's solution (BSP x nr)
+    auto apply_u = [&](int k, const T (&v)[16], const T *X) {
+        const int p = cta + k * G, rows = rows_of(p);
+        const int r = tid >> 2, part = tid & 3;  // 16 columns per thread
+        T s[BS_MAXR];
+#pragma unroll
+        for (int q = 0; q < BS_MAXR; q++) s[q] = T(0);
+        if (r < rows) {
 #pragma unroll
             for (int e = 0; e < 16; e++)
 #pragma unroll
@@ -313,6 +328,12 @@ __global__ void __launch_bounds__(BSP_THREADS) backsolve_persistent_kernel(BsPar
     for (int p_src = 0; p_src < nblk; p_src++) {
         const int buf = p_src & 1;
         T *X = xs + buf * BSP * BS_MAXR;
+        // the U tiles of the first pending owned blocks, before the wait
+        const int k_first = next;
+        T v[BSP_AHEAD][16];
+#pragma unroll
+        for (int j = 0; j < BSP_AHEAD; j++)
+            if (k_first + j < n_own) load_u(k_first + j, p_src, v[j]);
         if (p_src % G != cta) {
             // wait for the source block's publication, then read its x through L2
             if (tid == 0) {
@@ -336,16 +357,25 @@ __global__ void __launch_bounds__(BSP_THREADS) backsolve_persistent_kernel(BsPar
             }
             __syncthreads();
         }
-        const int k_first = next;
         if (k_first < n_own) {
-            update(k_first, p_src, X);
+            apply_u(k_first, v[0], X);
             if (cta + k_first * G == p_src + 1) {
                 __syncthreads();
                 solve(k_first, buf ^ 1);
                 next = k_first + 1;
             }
         }
-        for (int k = k_first + 1; k < n_own; k++) update(k, p_src, X);
+#pragma unroll
+        for (int j = 1; j < BSP_AHEAD; j++)
+            if (k_first + j < n_own) apply_u(k_first + j, v[j], X);
+        for (int k0 = k_first + BSP_AHEAD; k0 < n_own; k0 += BSP_AHEAD) {
+#pragma unroll
+            for (int j = 0; j < BSP_AHEAD; j++)
+                if (k0 + j < n_own) load_u(k0 + j, p_src, v[j]);
+#pragma unroll
+            for (int j = 0; j < BSP_AHEAD; j++)
+                if (k0 + j < n_own) apply_u(k0 + j, v[j], X);
+        }
         __syncthreads();  // X (this buffer) is overwritten two sources later
     }
 }
