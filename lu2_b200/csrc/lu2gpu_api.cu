@@ -1275,6 +1275,37 @@ static int left_looking_panels(int n, int nb)
 // column n) comes back, and pv[0..m) holds the last panel's pivot rows as in
 // the reference.  `recursive` is accepted for signature compatibility; the
 // GPU path is always the recursive one.  `awork` is not used.
+// Pageable host matrices at least this large are page-locked by lumcolumn
+// for the call (the copies then overlap the factorization).
+constexpr size_t HOST_REGISTER_MIN_BYTES = (size_t)2 << 30;
+
+// cudaHostRegister for the duration of one call: take() registers a range;
+// the destructor waits for the context's streams (copies of the range may
+// still be in flight after an error return) and unregisters it.
+struct HostRegistration {
+    lu2gpu_ctx *c;
+    void *ptr = nullptr;
+    explicit HostRegistration(lu2gpu_ctx *ctx) : c(ctx) {}
+    bool take(void *p, size_t bytes)
+    {
+        if (cudaHostRegister(p, bytes, cudaHostRegisterDefault) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        ptr = p;
+        return true;
+    }
+    ~HostRegistration()
+    {
+        if (!ptr) return;
+        cudaStreamSynchronize(c->stream);
+        if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
+        if (c->h2d_stream) cudaStreamSynchronize(c->h2d_stream);
+        cudaHostUnregister(ptr);
+        cudaGetLastError();
+    }
+};
+
 static int lumcolumn_host(int n, double *a, double *b, int m, int *pv)
 {
     lu2gpu_ctx *c = default_ctx();
@@ -1301,8 +1332,20 @@ static int lumcolumn_host(int n, double *a, double *b, int m, int *pv)
     // copy stream while the factorization continues; pageable memory would
     // make those copies block the enqueuing thread, so it is copied at the end
     cudaPointerAttributes pa{};
-    const bool pinned = cudaPointerGetAttributes(&pa, a) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+    bool pinned = cudaPointerGetAttributes(&pa, a) == cudaSuccess && pa.type == cudaMemoryTypeHost;
     cudaGetLastError();
+    // a large pageable matrix (lu2's main allocates it with malloc or from
+    // hugetlbfs, lu2.c:1245-1264) is page-locked for the duration of the call,
+    // so that it takes the overlapped path; LU2GPU_HOST_REGISTER=0 never, =1
+    // always, default from HOST_REGISTER_MIN_BYTES.  Unregistered on every
+    // return, after the streams that copy it are idle.
+    HostRegistration reg(c);
+    if (!pinned) {
+        const char *hr = getenv("LU2GPU_HOST_REGISTER");
+        const size_t bytes = (size_t)n * rdim * sizeof(double);
+        const bool want = hr ? atoi(hr) != 0 : bytes >= HOST_REGISTER_MIN_BYTES;
+        if (want && reg.take(a, bytes)) pinned = true;
+    }
     // nothing of an earlier call (one that may have failed half way) still in flight
     if (c->copy_stream) CU_TRY(cudaStreamSynchronize(c->copy_stream));
     if (c->h2d_stream) CU_TRY(cudaStreamSynchronize(c->h2d_stream));

@@ -208,6 +208,38 @@ def test_lumcolumn_left_looking_start_is_bit_identical(oracle, monkeypatch, n, n
     np.testing.assert_array_equal(pv_pin, pv_pg)
 
 
+def _host_memory_type(arr) -> int:
+    """cudaPointerAttributes.type of a host array (0: unregistered, 1: page-locked)."""
+    import ctypes
+    import glob
+
+    rt = ctypes.CDLL(sorted(glob.glob("/usr/local/cuda/lib64/libcudart.so*"))[0])
+    attr = (ctypes.c_int * 8)()
+    rc = rt.cudaPointerGetAttributes(ctypes.byref(attr), ctypes.c_void_p(arr.ctypes.data))
+    rt.cudaGetLastError()
+    return int(attr[0]) if rc == 0 else 0
+
+
+@pytest.mark.parametrize("n,nb", [(1500, 128), (700, 64)])
+def test_lumcolumn_registers_pageable_matrix_for_the_call(oracle, monkeypatch, n, nb):
+    """A pageable matrix page-locked by lumcolumn for the call (forced here
+    with LU2GPU_HOST_REGISTER=1; by default only from 2 GB) takes the
+    overlapped path and gives the pageable path's result bit for bit; the
+    array is unregistered again when the call returns."""
+    out = []
+    for reg in ("0", "1"):
+        monkeypatch.setenv("LU2GPU_HOST_REGISTER", reg)
+        a = oracle.randomsetmat(n, 21)
+        b = np.zeros(n)
+        pv = np.zeros(nb, dtype=np.int32)
+        assert _host_memory_type(a) == 0
+        assert lumcolumn(a, b, nb, pv, PIVOT_PARTIAL) == 0
+        assert _host_memory_type(a) == 0
+        out.append((a[:, : n + 1].copy(), b.copy(), pv.copy()))
+    for u, v in zip(out[0], out[1]):
+        np.testing.assert_array_equal(u, v)
+
+
 @pytest.mark.parametrize("n,nb", [(1, 16), (2, 16), (15, 16), (16, 16), (17, 16), (33, 16), (100, 32), (1000, 256),
                                   (777, 64)])
 def test_ragged_sizes_vs_lapack(ctx, oracle, n, nb):
