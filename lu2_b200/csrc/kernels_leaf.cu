@@ -58,26 +58,6 @@ __device__ __forceinline__ unsigned stamp_of(unsigned long long seq)
     return (unsigned)(seq % 4294967295ull) + 1u;
 }
 
-// a double as two stamped words (high half, low half)
-__device__ __forceinline__ void st_stamped(unsigned long long *p, unsigned tag, double x)
-{
-    const unsigned long long b = (unsigned long long)__double_as_longlong(x), t = (unsigned long long)tag << 32;
-    const unsigned long long hi = t | (b >> 32), lo = t | (b & 0xffffffffull);
-    asm volatile("st.relaxed.gpu.global.v2.u64 [%0], {%1, %2};" ::"l"(p), "l"(hi), "l"(lo) : "memory");
-}
-
-__device__ __forceinline__ void ld_pair(const unsigned long long *p, unsigned long long &a, unsigned long long &b)
-{
-    asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];" : "=l"(a), "=l"(b) : "l"(p) : "memory");
-}
-
-__device__ __forceinline__ bool stamped(unsigned long long w, unsigned tag) { return (unsigned)(w >> 32) == tag; }
-
-__device__ __forceinline__ double unstamp(unsigned long long hi, unsigned long long lo)
-{
-    return __longlong_as_double((long long)((hi << 32) | (lo & 0xffffffffull)));
-}
-
 // T = double (plain form) or float (the precision form's FP32 panel); the
 // exchanged candidate rows are carried as double, which holds either exactly.
 template <typename T>

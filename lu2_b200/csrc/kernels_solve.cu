@@ -158,14 +158,16 @@ static cudaError_t launch_backsolve_t(const T *a, long ld, int n, int nrhs, T *x
 // oriented, one warp per right-hand side), so the critical path per block is
 // one 64x64 product and one 64x64 solve.  Each block of U is read once: a
 // CTA issues the loads of the U tiles its next BSP_AHEAD pending blocks take
-// from a source before it waits for that source's flag, so that their DRAM
+// from a source before it waits for that source's x, so that their DRAM
 // latency overlaps the wait (the tiles do not depend on x).
-// Publication: the block's x rows, then a fence and a release store of the
-// call's epoch into the block's flag; readers acquire the flag (bounded wait)
-// and read x through L2.
+// Publication: the solving warps store the block's x straight from their
+// registers into the block's slot as stamped words (the call's epoch beside
+// each 32-bit half, no fence); a reader re-loads the slot's words until all
+// carry the epoch (bounded wait), which gives it x in the same round trip.
 constexpr int BSP = 64;          // rows per block
 constexpr int BSP_THREADS = 256;
-constexpr int BSP_AHEAD = 2;     // U tiles per CTA loaded before a source's flag is awaited
+constexpr int BSP_AHEAD = 2;     // U tiles per CTA loaded before a source's x is awaited
+static_assert(BS_SLOT_WORDS == BSP * BS_MAXR * 2, "an x slot holds a block's rows x right-hand sides as stamped pairs");
 
 template <typename T>
 struct BsParams {
@@ -175,22 +177,10 @@ struct BsParams {
     T *x;
     long ldx;
     int c0, nr;
-    unsigned *flags;
+    unsigned long long *xslots;  // [nblk][BS_SLOT_WORDS]: element (r, q) of a block at 2 (r BS_MAXR + q)
     unsigned epoch;
     int *status;
 };
-
-__device__ __forceinline__ unsigned bs_ld_acquire(const unsigned *p)
-{
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
-__device__ __forceinline__ void bs_st_release(unsigned *p, unsigned v)
-{
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
 
 template <typename T>
 __global__ void __launch_bounds__(BSP_THREADS, 2) backsolve_persistent_kernel(BsParams<T> P)
@@ -202,12 +192,10 @@ __global__ void __launch_bounds__(BSP_THREADS, 2) backsolve_persistent_kernel(Bs
     T *acc = reinterpret_cast<T *>(bsp_smem);      // [n_own][BSP][BS_MAXR]
     T *Ud = acc + (size_t)n_own * BSP * BS_MAXR;    // [BSP][BSP + 1]
     T *xs = Ud + BSP * (BSP + 1);                   // [2][BSP][BS_MAXR]
-    __shared__ int s_fail;
     // block p covers rows r0(p) .. r0(p) + rows(p) - 1
     auto r0_of = [&](int p) { return (nblk - 1 - p) * BSP; };
     auto rows_of = [&](int p) { return min(BSP, P.n - r0_of(p)); };
 
-    if (tid == 0) s_fail = 0;
     for (int k = 0; k < n_own; k++) {
         const int p = cta + k * G, r0 = r0_of(p), rows = rows_of(p);
         for (int e = tid; e < BSP * BS_MAXR; e += BSP_THREADS) {
@@ -239,7 +227,8 @@ __global__ void __launch_bounds__(BSP_THREADS, 2) backsolve_persistent_kernel(Bs
         asm volatile("cp.async.commit_group;" ::: "memory");
     };
 
-    // solve owned block k (all updates from the blocks below applied) into xs[buf] and x; publish
+    // solve owned block k (all updates from the blocks below applied) into
+    // xs[buf] and x; the solving warps publish it first
     auto solve = [&](int k, int buf) {
         const int p = cta + k * G, r0 = r0_of(p), rows = rows_of(p);
         asm volatile("cp.async.wait_group 0;" ::: "memory");
@@ -253,6 +242,9 @@ __global__ void __launch_bounds__(BSP_THREADS, 2) backsolve_persistent_kernel(Bs
                 if (lane < c) y0 -= Ud[lane * (BSP + 1) + c] * xc;
                 if (lane + 32 < c) y1 -= Ud[(lane + 32) * (BSP + 1) + c] * xc;
             }
+            unsigned long long *slot = P.xslots + (size_t)(nblk - 1 - p) * BS_SLOT_WORDS;
+            if (lane < rows) st_stamped(slot + 2 * (lane * BS_MAXR + warp), P.epoch, (double)y0);
+            if (lane + 32 < rows) st_stamped(slot + 2 * ((lane + 32) * BS_MAXR + warp), P.epoch, (double)y1);
             A[lane * BS_MAXR + warp] = y0;
             A[(lane + 32) * BS_MAXR + warp] = y1;
         }
@@ -265,27 +257,41 @@ __global__ void __launch_bounds__(BSP_THREADS, 2) backsolve_persistent_kernel(Bs
             if (r < rows && q < nr) P.x[(size_t)(r0 + r) * P.ldx + P.c0 + q] = v;
         }
         __syncthreads();
-        if (tid == 0) {
-            __threadfence();
-            bs_st_release(&P.flags[nblk - 1 - p], P.epoch);
-        }
         if (k + 1 < n_own) prefetch_diag(k + 1);
     };
 
     // thread (r, part) of owned block k's U tile for source p_src: row r,
-    // columns 16 part .. 16 part + 15 (zero outside the tile)
+    // the column pairs 8 j + 2 part, 8 j + 2 part + 1 (j = 0..7) as v[2j],
+    // v[2j+1] (zero outside the tile): the four threads of a row read 64
+    // contiguous bytes per load, with one 2-element vector load each where
+    // the matrix's alignment and row stride allow
+    const bool uvec = ((reinterpret_cast<uintptr_t>(P.a) & (2 * sizeof(T) - 1)) == 0) && ((P.ld & 1) == 0);
     auto load_u = [&](int k, int p_src, T (&v)[16]) {
         const int p = cta + k * G, r0 = r0_of(p), rows = rows_of(p);
         const int c0 = r0_of(p_src), cols = rows_of(p_src);
         const int r = tid >> 2, part = tid & 3;
         if (r < rows) {
-            const T *u = P.a + (size_t)(r0 + r) * P.ld + c0 + part * 16;
-            if (part * 16 + 16 <= cols) {
+            const T *u = P.a + (size_t)(r0 + r) * P.ld + c0 + 2 * part;
+            if (uvec && cols == BSP) {
 #pragma unroll
-                for (int e = 0; e < 16; e++) v[e] = __ldg(u + e);
+                for (int j = 0; j < 8; j++) {
+                    if constexpr (sizeof(T) == 8) {
+                        const double2 w = __ldg(reinterpret_cast<const double2 *>(u + 8 * j));
+                        v[2 * j] = w.x;
+                        v[2 * j + 1] = w.y;
+                    } else {
+                        const float2 w = __ldg(reinterpret_cast<const float2 *>(u + 8 * j));
+                        v[2 * j] = w.x;
+                        v[2 * j + 1] = w.y;
+                    }
+                }
             } else {
 #pragma unroll
-                for (int e = 0; e < 16; e++) v[e] = (part * 16 + e < cols) ? __ldg(u + e) : T(0);
+                for (int j = 0; j < 8; j++) {
+                    const int col = 8 * j + 2 * part;
+                    v[2 * j] = col < cols ? __ldg(u + 8 * j) : T(0);
+                    v[2 * j + 1] = col + 1 < cols ? __ldg(u + 8 * j + 1) : T(0);
+                }
             }
         } else {
 #pragma unroll
@@ -305,7 +311,7 @@ __global__ void __launch_bounds__(BSP_THREADS, 2) backsolve_persistent_kernel(Bs
             for (int e = 0; e < 16; e++)
 #pragma unroll
                 for (int q = 0; q < BS_MAXR; q++)
-                    if (q < nr) s[q] += v[e] * X[(part * 16 + e) * BS_MAXR + q];
+                    if (q < nr) s[q] += v[e] * X[(8 * (e >> 1) + 2 * part + (e & 1)) * BS_MAXR + q];
         }
 #pragma unroll
         for (int q = 0; q < BS_MAXR; q++) {
@@ -335,27 +341,41 @@ __global__ void __launch_bounds__(BSP_THREADS, 2) backsolve_persistent_kernel(Bs
         for (int j = 0; j < BSP_AHEAD; j++)
             if (k_first + j < n_own) load_u(k_first + j, p_src, v[j]);
         if (p_src % G != cta) {
-            // wait for the source block's publication, then read its x through L2
-            if (tid == 0) {
-                const unsigned *f = &P.flags[nblk - 1 - p_src];
-                unsigned spins = 0;
-                while (bs_ld_acquire(f) != P.epoch) {
-                    if ((++spins & 255u) == 0 &&
-                        (*(volatile int *)&P.status[1] != 0 || globaltimer_ns() - t0 > WAIT_LIMIT_NS)) {
-                        if (*(volatile int *)&P.status[1] == 0) record_error(P.status, ERR_BARRIER_TIMEOUT, 6);
-                        s_fail = 1;
-                        break;
+            // the source block's x from its slot: each thread re-loads its
+            // elements until they carry this call's epoch; the CTA agrees on
+            // completion, or on giving up, at one barrier per round
+            const unsigned long long *slot = P.xslots + (size_t)(nblk - 1 - p_src) * BS_SLOT_WORDS;
+            const int rows = rows_of(p_src);
+            constexpr int EPT = BSP * BS_MAXR / BSP_THREADS;  // elements per thread
+            unsigned todo = 0;
+#pragma unroll
+            for (int u = 0; u < EPT; u++) {
+                const int e = tid + u * BSP_THREADS, r = e / BS_MAXR, q = e % BS_MAXR;
+                if (r < rows && q < nr)
+                    todo |= 1u << u;
+                else
+                    X[e] = T(0);
+            }
+            for (unsigned round = 1;; round++) {
+#pragma unroll
+                for (int u = 0; u < EPT; u++) {
+                    if (!((todo >> u) & 1u)) continue;
+                    const int e = tid + u * BSP_THREADS;
+                    unsigned long long hi, lo;
+                    ld_pair(slot + 2 * e, hi, lo);
+                    if (stamped(hi, P.epoch) && stamped(lo, P.epoch)) {
+                        X[e] = (T)unstamp(hi, lo);
+                        todo &= ~(1u << u);
                     }
                 }
+                if (__syncthreads_and(todo == 0)) break;
+                const bool late = (round & 63u) == 0 && tid == 0 &&
+                                  (*(volatile int *)&P.status[1] != 0 || globaltimer_ns() - t0 > WAIT_LIMIT_NS);
+                if (__syncthreads_or(late)) {
+                    if (tid == 0 && *(volatile int *)&P.status[1] == 0) record_error(P.status, ERR_BARRIER_TIMEOUT, 6);
+                    return;
+                }
             }
-            __syncthreads();
-            if (s_fail) return;
-            const int r0 = r0_of(p_src), rows = rows_of(p_src);
-            for (int e = tid; e < BSP * BS_MAXR; e += BSP_THREADS) {
-                const int r = e / BS_MAXR, q = e % BS_MAXR;
-                X[e] = (r < rows && q < nr) ? __ldcg(P.x + (size_t)(r0 + r) * P.ldx + P.c0 + q) : T(0);
-            }
-            __syncthreads();
         }
         if (k_first < n_own) {
             apply_u(k_first, v[0], X);
@@ -415,7 +435,7 @@ static cudaError_t launch_backsolve_persistent(const T *a, long ld, int n, int n
     if (G == 0) return cudaSuccess;  // the blocked launches take it
     (void)n_own;
     for (int c0 = 0; c0 < nrhs; c0 += BS_MAXR) {
-        BsParams<T> P{a, ld, n, nblk, x, ldx, c0, nrhs - c0 < BS_MAXR ? nrhs - c0 : BS_MAXR, bs.flags, 0u, bs.status};
+        BsParams<T> P{a, ld, n, nblk, x, ldx, c0, nrhs - c0 < BS_MAXR ? nrhs - c0 : BS_MAXR, bs.xslots, 0u, bs.status};
         P.epoch = ++*bs.epoch;
         if (P.epoch == 0) P.epoch = ++*bs.epoch;
         void *args[] = {&P};
@@ -432,7 +452,7 @@ template <typename T>
 static cudaError_t launch_backsolve_any(const T *a, long ld, int n, int nrhs, T *x, long ldx, const BsBuffers *bs,
                                        cudaStream_t st)
 {
-    if (bs && bs->flags && n >= BSP_PERSISTENT_MIN_N) {
+    if (bs && bs->xslots && n >= BSP_PERSISTENT_MIN_N) {
         bool used = false;
         cudaError_t e = launch_backsolve_persistent(a, ld, n, nrhs, x, ldx, *bs, st, &used);
         if (e != cudaSuccess || used) return e;

@@ -118,8 +118,8 @@ struct lu2gpu_ctx {
     // workspaces of the precision form (lu2gpu_mixed_solve), allocated on first use
     struct MixedWork *mx = nullptr;
     // publication flags of the persistent back substitution (one per 64-row block)
-    unsigned *d_bsflags = nullptr;
-    int bsflags_cap = 0;
+    unsigned long long *d_bsx = nullptr;  // stamped x slots of the persistent back solve
+    int bsx_cap = 0;
     unsigned bs_epoch = 0;
     BsBuffers bs{};
 };
@@ -132,22 +132,22 @@ static const BsBuffers *bs_buffers(lu2gpu_ctx *c, int n)
 {
     if (c->fixed_scratch) return nullptr;
     const int need = (n + 63) / 64;
-    if (need > c->bsflags_cap) {
-        cudaFree(c->d_bsflags);
-        c->d_bsflags = nullptr;
-        c->bsflags_cap = 0;
+    if (need > c->bsx_cap) {
+        cudaFree(c->d_bsx);
+        c->d_bsx = nullptr;
+        c->bsx_cap = 0;
         const int cap = need + 256;
-        if (cudaMalloc(&c->d_bsflags, (size_t)cap * sizeof(unsigned)) != cudaSuccess ||
-            cudaMemsetAsync(c->d_bsflags, 0, (size_t)cap * sizeof(unsigned), c->stream) != cudaSuccess) {
+        const size_t bytes = (size_t)cap * BS_SLOT_WORDS * sizeof(unsigned long long);
+        if (cudaMalloc(&c->d_bsx, bytes) != cudaSuccess || cudaMemsetAsync(c->d_bsx, 0, bytes, c->stream) != cudaSuccess) {
             cudaGetLastError();
-            cudaFree(c->d_bsflags);
-            c->d_bsflags = nullptr;
+            cudaFree(c->d_bsx);
+            c->d_bsx = nullptr;
             return nullptr;
         }
-        c->bsflags_cap = cap;
+        c->bsx_cap = cap;
     }
-    c->bs.flags = c->d_bsflags;
-    c->bs.cap = c->bsflags_cap;
+    c->bs.xslots = c->d_bsx;
+    c->bs.cap = c->bsx_cap;
     c->bs.epoch = &c->bs_epoch;
     c->bs.status = c->d_status;
     return &c->bs;
@@ -265,7 +265,7 @@ extern "C" int lu2gpu_destroy(lu2gpu_ctx *c)
     if (c->ev_panel) cudaEventDestroy(c->ev_panel);
     cudaFree(c->d_ipiv);
     cudaFree(c->d_dinv);
-    cudaFree(c->d_bsflags);
+    cudaFree(c->d_bsx);
     for (int i = 0; i < 4; i++) cudaFree(c->d_stage[i]);
     if (c->copy_stream) {
         cudaStreamSynchronize(c->copy_stream);

@@ -44,6 +44,29 @@ __device__ __forceinline__ void record_error(int *status, int bit, int where)
     if (atomicOr(&status[1], bit) == 0) atomicExch(&status[2], where);
 }
 
+// Stamped publication between CTAs without fences: a double travels as two
+// 64-bit words, each a 32-bit stamp (the publication's tag, never 0) beside
+// 32 bits of the value; a reader re-loads until both words carry the tag it
+// waits for (aligned 64-bit accesses are single-copy atomic).
+__device__ __forceinline__ void st_stamped(unsigned long long *p, unsigned tag, double x)
+{
+    const unsigned long long b = (unsigned long long)__double_as_longlong(x), t = (unsigned long long)tag << 32;
+    const unsigned long long hi = t | (b >> 32), lo = t | (b & 0xffffffffull);
+    asm volatile("st.relaxed.gpu.global.v2.u64 [%0], {%1, %2};" ::"l"(p), "l"(hi), "l"(lo) : "memory");
+}
+
+__device__ __forceinline__ void ld_pair(const unsigned long long *p, unsigned long long &a, unsigned long long &b)
+{
+    asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];" : "=l"(a), "=l"(b) : "l"(p) : "memory");
+}
+
+__device__ __forceinline__ bool stamped(unsigned long long w, unsigned tag) { return (unsigned)(w >> 32) == tag; }
+
+__device__ __forceinline__ double unstamp(unsigned long long hi, unsigned long long lo)
+{
+    return __longlong_as_double((long long)((hi << 32) | (lo & 0xffffffffull)));
+}
+
 // (value, row) ordering for the pivot search: larger |a| wins, ties go to the
 // lower row index (cblas_idamax semantics, lu2tlib.c:47).
 __device__ __forceinline__ bool argmax_better(double v1, int i1, double v2, int i2)
@@ -143,12 +166,14 @@ cudaError_t launch_transpose(const double *in, long ldi, double *out, long ldo, 
 
 // x = U'^{-1} y for the unit upper triangle of a[0..n)[0..n) (lu2's backward_sub,
 // lu2.c:110-116); y (n x nrhs, row stride ldx) is overwritten by x.  For lu2's
-// own layout x = a + n, ldx = ld.  With bs (flags for n / 64 blocks, zeroed
-// once; a host epoch counter; the status words) and n >= BSP_PERSISTENT_MIN_N
-// one persistent cooperative launch per 8 right-hand sides does it; otherwise
-// blocked launches (one per 128-row block and one per update).
+// own layout x = a + n, ldx = ld.  With bs (a stamped x slot for each of the
+// n / 64 blocks, zeroed once; a host epoch counter; the status words) and
+// n >= BSP_PERSISTENT_MIN_N one persistent cooperative launch per 8
+// right-hand sides does it; otherwise blocked launches (one per 128-row block
+// and one per update).
+constexpr int BS_SLOT_WORDS = 64 * 8 * 2;  // 64 rows x 8 right-hand sides, two stamped words each
 struct BsBuffers {
-    unsigned *flags = nullptr;  // [cap], zeroed at allocation
+    unsigned long long *xslots = nullptr;  // [cap][BS_SLOT_WORDS], zeroed at allocation
     int cap = 0;
     unsigned *epoch = nullptr;  // host-side counter, advanced per launch
     int *status = nullptr;
