@@ -285,15 +285,17 @@ __device__ void batch_solve_blocked(double *A, long ld, int n, int nrhs, int pw,
     }
     // back substitution with the unit upper factor (lu2.c:110-116), blocked by
     // 32 rows: y (n x nrhs) and each 32 x 32 diagonal block in shared memory
-    // (reusing the panel's space), the rows above updated from their 32-wide
-    // row segments
+    // (reusing the panel's space); warp 0 solves the diagonal block
+    // warp-synchronously (lane = row, the solved value passed by shuffle),
+    // then the rows above are updated from their 32-wide row segments, four
+    // threads per row on interleaved 16-byte column pairs
     double *Y = P;
     double *Ud = P + (size_t)n * nrhs;  // 32 x 33
     for (int idx = tid; idx < n * nrhs; idx += T) {
         const int r = idx / nrhs, q = idx - r * nrhs;
         Y[idx] = A[(size_t)r * ld + n + q];
     }
-    __syncthreads();
+    const int warp = tid >> 5, lane = tid & 31, part = tid & 3;
     for (int jb = ((n - 1) / 32) * 32; jb >= 0; jb -= 32) {
         const int je = min(jb + 32, n), bw = je - jb;
         for (int idx = tid; idx < bw * bw; idx += T) {
@@ -301,21 +303,49 @@ __device__ void batch_solve_blocked(double *A, long ld, int n, int nrhs, int pw,
             Ud[i * 33 + j] = A[(size_t)(jb + i) * ld + jb + j];
         }
         __syncthreads();
-        for (int j = bw - 1; j >= 1; j--) {
-            for (int idx = tid; idx < j * nrhs; idx += T) {
-                const int i = idx / nrhs, q = idx - i * nrhs;
-                Y[(jb + i) * nrhs + q] -= Ud[i * 33 + j] * Y[(jb + j) * nrhs + q];
-            }
-            __syncthreads();
-        }
-        for (int i = tid; i < jb; i += T) {
-            const double *row = A + (size_t)i * ld + jb;
-            double u[32];
-            for (int j = 0; j < bw; j++) u[j] = row[j];
+        if (warp == 0) {
             for (int q = 0; q < nrhs; q++) {
-                double s = 0.0;
-                for (int j = 0; j < bw; j++) s = fma(u[j], Y[(jb + j) * nrhs + q], s);
-                Y[i * nrhs + q] -= s;
+                double y = lane < bw ? Y[(jb + lane) * nrhs + q] : 0.0;
+                for (int j = bw - 1; j >= 1; j--) {
+                    const double yj = __shfl_sync(0xffffffffu, y, j);
+                    if (lane < j) y -= Ud[lane * 33 + j] * yj;
+                }
+                if (lane < bw) Y[(jb + lane) * nrhs + q] = y;
+            }
+        }
+        __syncthreads();
+        // (jb, ld and the system's base are even / 16-byte aligned: jb > 0 rows
+        // take one 16-byte load per column pair)
+        for (int i0 = 0; i0 < jb; i0 += T >> 2) {
+            const int i = i0 + (tid >> 2);
+            double u[8];
+#pragma unroll
+            for (int e = 0; e < 8; e++) u[e] = 0.0;
+            if (i < jb) {
+                const double *row = A + (size_t)i * ld + jb + 2 * part;
+#pragma unroll
+                for (int jj = 0; jj < 4; jj++) {
+                    const int c = 8 * jj + 2 * part;
+                    if (c + 1 < bw) {
+                        const double2 w = *reinterpret_cast<const double2 *>(row + 8 * jj);
+                        u[2 * jj] = w.x;
+                        u[2 * jj + 1] = w.y;
+                    } else if (c < bw) {
+                        u[2 * jj] = row[8 * jj];
+                    }
+                }
+            }
+            for (int q = 0; q < nrhs; q++) {
+                double sacc = 0.0;
+#pragma unroll
+                for (int jj = 0; jj < 4; jj++) {
+                    const int c = 8 * jj + 2 * part;
+                    if (c < bw) sacc = fma(u[2 * jj], Y[(jb + c) * nrhs + q], sacc);
+                    if (c + 1 < bw) sacc = fma(u[2 * jj + 1], Y[(jb + c + 1) * nrhs + q], sacc);
+                }
+                sacc += __shfl_xor_sync(0xffffffffu, sacc, 1);
+                sacc += __shfl_xor_sync(0xffffffffu, sacc, 2);
+                if (part == 0 && i < jb) Y[i * nrhs + q] -= sacc;
             }
         }
         __syncthreads();
