@@ -145,7 +145,7 @@ def ref_run(ref, n, nb, seed, runs, orc=None):
 
 
 def c1_baseline(cores: int, runs: int = 5) -> dict:
-    """BASELINE config 1, the reference CPU lu2 (nompi) at N = 2048, nb = 64:
+    """The reference CPU lu2 (nompi) on its own CPU-sized case, N = 2048, nb = 64:
     shipped and pivot-fixed builds, seeds 1 and 12345, OpenBLAS on every core
     with one OpenMP thread (the fastest split), median of `runs`; plus the
     default split (OpenMP and OpenBLAS both on every core), timed once."""
@@ -171,7 +171,7 @@ def c1_baseline(cores: int, runs: int = 5) -> dict:
 def cpu_reference_gflops(n: int, nb: int, runs: int) -> dict:
     """The reference's own lumcolumn on the host cores (oracle/_ref): the
     bounded N = n sample of the workload (shipped build, the baseline of
-    record; the pivot-fixed build beside it) and BASELINE config 1 (c1_*)."""
+    record; the pivot-fixed build beside it) and the N = 2048, nb = 64 case (c1_*)."""
     cores = os.cpu_count() or 1
     from oracle.oracle import OracleLib, RefLib
 

@@ -4,7 +4,7 @@
  * oracle restatement against the reference itself, and bench.py can time the
  * reference's own CPU path.
  *
- * TEST / BASELINE INFRASTRUCTURE ONLY: never linked into the product.
+ * TEST AND CPU-BASELINE INFRASTRUCTURE ONLY: never linked into the product.
  *
  * Entry points used from the reference (file:line in telmin/lu2):
  *   randomsetmat                     lu2.c:70-85
