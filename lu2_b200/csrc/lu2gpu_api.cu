@@ -2558,7 +2558,7 @@ extern "C" int lu2gpu_batch_autotune(lu2gpu_batch *b, int *params_out)
                 if (batch_configure(b, bt, bp, bc)) continue;  // does not fit
                 float ms = 0.f;
                 if ((rc = batch_time3(b, st, e0, e1, &ms))) break;
-                if (ms < best) {
+                if (ms < 0.99f * best) {  // a bucket leaves the launch's width only for a clear gain
                     best = ms;
                     keep = cand_pw[pi];
                 }
