@@ -117,8 +117,8 @@ struct lu2gpu_ctx {
     long launches[PH_COUNT] = {};
     // workspaces of the precision form (lu2gpu_mixed_solve), allocated on first use
     struct MixedWork *mx = nullptr;
-    // publication flags of the persistent back substitution (one per 64-row block)
-    unsigned long long *d_bsx = nullptr;  // stamped x slots of the persistent back solve
+    // stamped x slots of the persistent back substitution (one per 64-row block)
+    unsigned long long *d_bsx = nullptr;
     int bsx_cap = 0;
     unsigned bs_epoch = 0;
     BsBuffers bs{};
@@ -126,8 +126,8 @@ struct lu2gpu_ctx {
 
 static void free_mixed(lu2gpu_ctx *c);
 
-// the back substitution's flags for an order-n system (null when they cannot
-// be had: the blocked launches then do it)
+// the back substitution's x slots for an order-n system (null when they
+// cannot be had: the blocked launches then do it)
 static const BsBuffers *bs_buffers(lu2gpu_ctx *c, int n)
 {
     if (c->fixed_scratch) return nullptr;
