@@ -110,6 +110,8 @@ __device__ __forceinline__ void batch_dmma(double (&c)[4], double a0, double a1,
 __device__ void batch_solve_blocked(double *A, long ld, int n, int nrhs, int pw, double *P, double *U, int *piv,
                                     double *dinv, int *info)
 {
+    __shared__ double s_pv[4];  // the panel warps' pivot candidates
+    __shared__ int s_pi[4];
     const int nc = n + nrhs, T = blockDim.x, tid = threadIdx.x;
     // panel row stride pw + 1 (odd): the lanes of the panel factorization, one
     // row each, fall into different banks
@@ -132,15 +134,20 @@ __device__ void batch_solve_blocked(double *A, long ld, int n, int nrhs, int pw,
             }
         }
         __syncthreads();
-        // the panel factored by warp 0 alone, warp-synchronously: one lane per
-        // row (rows lane, lane+32, ...), no CTA barrier per column; per element
-        // the same operations as a CTA-wide elimination
-        if (tid < 32) {
-            const int lane = tid;
+        // the panel factored by the first NWP warps (up to 4): thread pt owns
+        // the rows c + pt + k S (S = 32 NWP) of column c -- the same rows for
+        // the pivot search of column c and the rank-1 step of column c - 1,
+        // so it only reads rows it wrote itself; two named barriers of the S
+        // threads per column (candidates in, pivot row swapped and scaled),
+        // no CTA barrier; per element the same operations as a CTA-wide
+        // elimination
+        const int nwp = min(4, T >> 5), S = 32 * nwp;
+        if (tid < S) {
+            const int lane = tid & 31, pw_ = tid >> 5;
             for (int c = 0; c < w; c++) {
                 double v = -1.0;
                 int p = INT_MAX;
-                for (int r = c + lane; r < rows; r += 32) {
+                for (int r = c + tid; r < rows; r += S) {
                     const double a = fabs(P[r * ps + c]);
                     if (a > v) {
                         v = a;
@@ -148,34 +155,48 @@ __device__ void batch_solve_blocked(double *A, long ld, int n, int nrhs, int pw,
                     }
                 }
                 warp_argmax(v, p);
-                if (p == INT_MAX) p = c;
-                if (lane == 0) piv[c] = p;
-                if (p != c)
-                    for (int j = lane; j < w; j += 32) {
-                        const double t = P[c * ps + j];
-                        P[c * ps + j] = P[p * ps + j];
-                        P[p * ps + j] = t;
+                if (lane == 0) {
+                    s_pv[pw_] = v;
+                    s_pi[pw_] = p;
+                }
+                asm volatile("bar.sync 1, %0;" ::"r"(S) : "memory");
+                v = s_pv[0];
+                p = s_pi[0];
+                for (int q = 1; q < nwp; q++)
+                    if (argmax_better(s_pv[q], s_pi[q], v, p)) {
+                        v = s_pv[q];
+                        p = s_pi[q];
                     }
-                __syncwarp();
-                const double d = P[c * ps + c];
-                const bool zero = (d == 0.0);
+                if (p == INT_MAX) p = c;
+                if (tid < 32) {
+                    if (lane == 0) piv[c] = p;
+                    if (p != c)
+                        for (int j = lane; j < w; j += 32) {
+                            const double t = P[c * ps + j];
+                            P[c * ps + j] = P[p * ps + j];
+                            P[p * ps + j] = t;
+                        }
+                    __syncwarp();
+                    const double d = P[c * ps + c];
+                    const bool zero = (d == 0.0);
+                    const double inv = zero ? 1.0 : 1.0 / d;
+                    if (lane == 0) dinv[c] = inv;
+                    __syncwarp();  // every lane has read the pivot before it is scaled
+                    if (!zero)
+                        for (int j = lane; j < w; j += 32)
+                            if (j != c) P[c * ps + j] *= inv;
+                }
+                asm volatile("bar.sync 1, %0;" ::"r"(S) : "memory");
+                const bool zero = (P[c * ps + c] == 0.0);
                 if (zero && !first_zero) first_zero = k0 + c + 1;
-                const double inv = zero ? 1.0 : 1.0 / d;
-                if (lane == 0) dinv[c] = inv;
-                __syncwarp();  // every lane has read the pivot before it is scaled
                 if (!zero)
-                    for (int j = lane; j < w; j += 32)
-                        if (j != c) P[c * ps + j] *= inv;
-                __syncwarp();
-                if (!zero)
-                    for (int r = c + 1 + lane; r < rows; r += 32) {
+                    for (int r = c + 1 + tid; r < rows; r += S) {
                         const double l = P[r * ps + c];
                         for (int j = c + 1; j < w; j++) P[r * ps + j] -= l * P[c * ps + j];
                     }
-                __syncwarp();
             }
         }
-        __syncthreads();  // (first_zero is tracked by warp 0, whose thread 0 reports it)
+        __syncthreads();  // (first_zero is tracked by the panel threads; thread 0 reports it)
         for (int idx = tid; idx < rows * w; idx += T) {
             const int r = idx / w, c = idx - r * w;
             A[(size_t)(k0 + r) * ld + k0 + c] = P[r * ps + c];
