@@ -269,6 +269,8 @@ typedef struct lu2gpu_batch lu2gpu_batch;
 /* Describe count systems (orders n[i] <= 4096, nrhs[i] <= 64 right-hand
  * sides; nrhs may be NULL for one each) and allocate their packed storage. */
 int lu2gpu_batch_create(lu2gpu_ctx *ctx, int count, const int *n, const int *nrhs, lu2gpu_batch **out);
+/* Frees the batch; call it before lu2gpu_destroy of the batch's context (the
+ * batch's memory and streams belong to that context). */
 int lu2gpu_batch_destroy(lu2gpu_batch *b);
 /* Device pointer to system i's augmented matrix and its row stride. */
 int lu2gpu_batch_system(lu2gpu_batch *b, int i, double **a, long *ld);

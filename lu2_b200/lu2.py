@@ -11,11 +11,32 @@ Every call goes through the C ABI; there is no CPU path.  Failures raise
 """
 from __future__ import annotations
 
+import atexit
 import ctypes as C
+import sys
+import weakref
 
 import numpy as np
 
 from . import _lib
+
+# Contexts and batches still open when the interpreter exits are closed by an
+# exit hook (batches first: a batch uses its context), while the CUDA runtime
+# is still up; a finalizer that runs later does nothing.
+_LIVE_BATCHES: "weakref.WeakSet" = weakref.WeakSet()
+_LIVE_CONTEXTS: "weakref.WeakSet" = weakref.WeakSet()
+
+
+def _close_live() -> None:
+    for group in (_LIVE_BATCHES, _LIVE_CONTEXTS):
+        for obj in list(group):
+            try:
+                obj.close()
+            except Exception:
+                pass
+
+
+atexit.register(_close_live)
 
 PIVOT_REF = 0
 PIVOT_PARTIAL = 1
@@ -124,6 +145,7 @@ class Context:
         self._h = C.c_void_p()
         _check("lu2gpu_create", lib().lu2gpu_create(C.byref(self._h), device))
         self.device = device
+        _LIVE_CONTEXTS.add(self)
 
     def close(self) -> None:
         if self._h:
@@ -131,6 +153,8 @@ class Context:
             self._h = C.c_void_p()
 
     def __del__(self):
+        if sys.is_finalizing():
+            return
         try:
             self.close()
         except Exception:
@@ -282,16 +306,21 @@ class Batch:
         self.n = np.ascontiguousarray(n, dtype=np.int32)
         self.nrhs = np.ascontiguousarray(nrhs if nrhs is not None else np.ones_like(self.n), dtype=np.int32)
         self.count = len(self.n)
+        self._ctx = ctx  # the batch's device memory and streams belong to this context
         self._h = C.c_void_p()
         _check("lu2gpu_batch_create", lib().lu2gpu_batch_create(ctx.handle, self.count, _ptr(self.n),
                                                                 _ptr(self.nrhs), C.byref(self._h)))
+        _LIVE_BATCHES.add(self)
 
     def close(self) -> None:
         if self._h:
-            lib().lu2gpu_batch_destroy(self._h)
+            if self._ctx.handle:
+                lib().lu2gpu_batch_destroy(self._h)
             self._h = C.c_void_p()
 
     def __del__(self):
+        if sys.is_finalizing():
+            return
         try:
             self.close()
         except Exception:

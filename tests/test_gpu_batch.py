@@ -221,3 +221,24 @@ def test_batch_fp32_ir_rejects_many_rhs(ctx):
     with pytest.raises(L.Lu2GpuError):
         b.set_mode(L.BATCH_FP32_IR, 10)
     b.close()
+
+
+def test_objects_left_open_at_exit_are_closed_in_order():
+    """A script that leaves a context and a batch open (module globals) exits
+    cleanly: the binding closes batches before contexts while the CUDA
+    runtime is still up, and a batch keeps its context alive."""
+    import os
+    import subprocess
+    import sys
+
+    code = ("import numpy as np, lu2_b200 as L\n"
+            "ctx = L.Context(0)\n"
+            "b = L.Batch(ctx, np.array([40, 300], dtype=np.int32))\n"
+            "b.generate(1)\n"
+            "assert (b.solve() == 0).all()\n"
+            "ctx2 = L.Context(0)\n"
+            "b2 = L.Batch(ctx2, np.array([17], dtype=np.int32))\n"
+            "del ctx2\n")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", code], cwd=root, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, (r.returncode, r.stderr[-2000:])
