@@ -106,9 +106,50 @@ __device__ __forceinline__ void batch_dmma(double (&c)[4], double a0, double a1,
         : "d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(b0), "d"(b1));
 }
 
+// The row exchanges of one panel composed into a plan: U row q takes the
+// content of panel row blk[q], and the rows ext_row[e] >= w take the old
+// content of U row ext_src[e] (every displaced row receives a U row, since
+// each exchange moves row c < w).
+struct BatchPlan {
+    int blk[64];
+    int ext_row[64];
+    int ext_src[64];
+    int next;
+};
+
+// warp 0, once the pivot p of column c is known: compose c <-> p into the
+// plan (the rows >= w already displaced are searched by the whole warp)
+__device__ __forceinline__ void batch_plan_step(BatchPlan &s, int c, int p, int w, int lane)
+{
+    const int ne = s.next;
+    unsigned hit = 0;
+    for (int e0 = 0; e0 < ne; e0 += 32) {
+        const unsigned b = __ballot_sync(0xffffffffu, e0 + lane < ne && s.ext_row[e0 + lane] == p);
+        if (b && !hit) hit = (unsigned)(e0 + __ffs(b));  // index + 1
+    }
+    if (lane == 0) {
+        const int xc = s.blk[c];
+        if (p < w) {
+            s.blk[c] = s.blk[p];
+            s.blk[p] = xc;
+        } else if (p != c) {
+            int e = (int)hit - 1;
+            if (!hit) {
+                e = ne;
+                s.ext_row[e] = p;
+                s.ext_src[e] = p;
+                s.next = e + 1;
+            }
+            s.blk[c] = s.ext_src[e];
+            s.ext_src[e] = xc;
+        }
+    }
+    __syncwarp();
+}
+
 // blocked LU in global memory (L2-resident), panel of pw columns in shared memory
 __device__ void batch_solve_blocked(double *A, long ld, int n, int nrhs, int pw, double *P, double *U, int *piv,
-                                    double *dinv, int *info)
+                                    double *dinv, BatchPlan &plan, int *info)
 {
     __shared__ double s_pv[4];  // the panel warps' pivot candidates
     __shared__ int s_pi[4];
@@ -144,6 +185,11 @@ __device__ void batch_solve_blocked(double *A, long ld, int n, int nrhs, int pw,
         const int nwp = min(4, T >> 5), S = 32 * nwp;
         if (tid < S) {
             const int lane = tid & 31, pw_ = tid >> 5;
+            if (tid < 32) {
+                for (int q = lane; q < w; q += 32) plan.blk[q] = q;
+                if (lane == 0) plan.next = 0;
+                __syncwarp();
+            }
             for (int c = 0; c < w; c++) {
                 double v = -1.0;
                 int p = INT_MAX;
@@ -185,6 +231,7 @@ __device__ void batch_solve_blocked(double *A, long ld, int n, int nrhs, int pw,
                     if (!zero)
                         for (int j = lane; j < w; j += 32)
                             if (j != c) P[c * ps + j] *= inv;
+                    batch_plan_step(plan, c, p, w, lane);
                 }
                 asm volatile("bar.sync 1, %0;" ::"r"(S) : "memory");
                 const bool zero = (P[c * ps + c] == 0.0);
@@ -202,22 +249,31 @@ __device__ void batch_solve_blocked(double *A, long ld, int n, int nrhs, int pw,
             A[(size_t)(k0 + r) * ld + k0 + c] = P[r * ps + c];
         }
         __syncthreads();
-        // right part: exchanges with 1/pivot scaling, then the unit-lower solve
-        // of the U block rows, one thread per column (lu2.c:524-581)
-        const int cs = k0 + w;
+        // right part: the composed exchanges with 1/pivot scaling, then the
+        // unit-lower solve of the U block rows, one thread per column
+        // (lu2.c:524-581).  The gathers are issued 16 at a time, then the
+        // displaced rows (loaded before U overwrites the rows they come from,
+        // stored after every gather, since a gathered row may be one of them)
+        const int cs = k0 + w, ne = plan.next;
         for (int j = cs + tid; j < nc; j += T) {
             double x[64];
-            for (int c = 0; c < w; c++) {
-                const int p = piv[c];
-                double *rc = A + (size_t)(k0 + c) * ld + j;
-                double vc = *rc;
-                if (p != c) {
-                    double *rp = A + (size_t)(k0 + p) * ld + j;
-                    const double vp = *rp;
-                    *rp = vc;
-                    vc = vp;
-                }
-                x[c] = vc * dinv[c];
+            for (int q0 = 0; q0 < w; q0 += 16) {
+                double v[16];
+#pragma unroll
+                for (int u = 0; u < 16; u++)
+                    v[u] = q0 + u < w ? A[(size_t)(k0 + plan.blk[q0 + u]) * ld + j] : 0.0;
+#pragma unroll
+                for (int u = 0; u < 16; u++)
+                    if (q0 + u < w) x[q0 + u] = v[u] * dinv[q0 + u];
+            }
+            for (int e0 = 0; e0 < ne; e0 += 16) {
+                double v[16];
+#pragma unroll
+                for (int u = 0; u < 16; u++)
+                    v[u] = e0 + u < ne ? A[(size_t)(k0 + plan.ext_src[e0 + u]) * ld + j] : 0.0;
+#pragma unroll
+                for (int u = 0; u < 16; u++)
+                    if (e0 + u < ne) A[(size_t)(k0 + plan.ext_row[e0 + u]) * ld + j] = v[u];
             }
             for (int r = 1; r < w; r++) {
                 double s = x[r];
@@ -385,6 +441,7 @@ __global__ void __launch_bounds__(512, 2) batch_lu_kernel(double *data, const Ba
     __shared__ int s_next;
     __shared__ int s_piv[64];
     __shared__ double s_dinv[64];
+    __shared__ BatchPlan s_plan;
     for (;;) {
         if (threadIdx.x == 0) s_next = atomicAdd(counter, 1);
         __syncthreads();
@@ -401,7 +458,7 @@ __global__ void __launch_bounds__(512, 2) batch_lu_kernel(double *data, const Ba
             // width when its size bucket has one
             const int pwi = S.pw ? S.pw : pw;
             batch_solve_blocked(A, S.ld, S.n, S.nrhs, pwi, bsm, bsm + (size_t)S.n * (pwi + BATCH_PANEL_PAD), s_piv,
-                                s_dinv, info + i);
+                                s_dinv, s_plan, info + i);
         }
         __syncthreads();
     }
