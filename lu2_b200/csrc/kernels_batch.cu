@@ -284,7 +284,7 @@ __device__ void batch_solve_blocked(double *A, long ld, int n, int nrhs, int pw,
         }
         __syncthreads();
         // trailing update A[k0+w.., cs..] -= L21 U12 on the FP64 tensor cores
-        // (mma.sync m16n8k8 f64), in 64-column chunks of U12 staged in shared
+        // (mma.sync m16n8k8 f64), in BATCH_U_CHUNK-column chunks of U12 staged in shared
         // memory; a warp takes 16 x 32 units (two per chunk row strip): C
         // fragments from global memory, -L21 fragments from the panel, U12
         // fragments from the chunk, K padded to a multiple of 8 with zeros
@@ -292,16 +292,17 @@ __device__ void batch_solve_blocked(double *A, long ld, int n, int nrhs, int pw,
         const int warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3, nwarps = T >> 5;
         const int ksteps = (w + 7) >> 3;
         const bool even = (cs & 1) == 0;  // 16-byte C accesses need an even column (always so: w = pw here)
-        for (int c0 = cs; c0 < nc && h > 0; c0 += 64) {
-            const int cw = min(64, nc - c0);
-            for (int idx = tid; idx < pw * 64; idx += T) {
-                const int l = idx >> 6, c = idx & 63;
+        for (int c0 = cs; c0 < nc && h > 0; c0 += BATCH_U_CHUNK) {
+            const int cw = min(BATCH_U_CHUNK, nc - c0);
+            for (int idx = tid; idx < pw * BATCH_U_CHUNK; idx += T) {
+                const int l = idx / BATCH_U_CHUNK, c = idx % BATCH_U_CHUNK;
                 U[l * BATCH_U_STRIDE + c] = (l < w && c < cw) ? A[(size_t)(k0 + l) * ld + c0 + c] : 0.0;
             }
             __syncthreads();
-            const int units = ((h + 15) >> 4) * 2;
+            constexpr int HALVES = BATCH_U_CHUNK / 32;  // 32-column halves of a warp's 16-row strip
+            const int units = ((h + 15) >> 4) * HALVES;
             for (int u = warp; u < units; u += nwarps) {
-                const int r0 = (u >> 1) << 4, cb = (u & 1) << 5;  // strip rows r0.., chunk columns cb..cb+31
+                const int r0 = (u / HALVES) << 4, cb = (u % HALVES) << 5;  // strip rows r0.., chunk columns cb..cb+31
                 const int rl = r0 + g, rh = rl + 8;                // rows (of the trailing block) of c0,c1 / c2,c3
                 double acc[4][4];
 #pragma unroll
