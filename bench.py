@@ -976,7 +976,7 @@ def main() -> int:
                "steps": len(ts), "api": "lumcolumn() C entry point, pinned host buffers"}
         del host, bvec
         # the same on pageable host memory, as lu2's main allocates a
-        # (malloc, lu2.c:1261-1262): one copy in before, one copy out after
+        # (malloc, lu2.c:1261-1262): lumcolumn page-locks it for the call
         if not args.no_e2e_pageable:
             hp = np.empty((n, n + 16))
             bp = np.empty(n)
