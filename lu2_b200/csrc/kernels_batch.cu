@@ -106,47 +106,6 @@ __device__ __forceinline__ void batch_dmma(double (&c)[4], double a0, double a1,
         : "d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(b0), "d"(b1));
 }
 
-// The row exchanges of one panel composed into a plan: U row q takes the
-// content of panel row blk[q], and the rows ext_row[e] >= w take the old
-// content of U row ext_src[e] (every displaced row receives a U row, since
-// each exchange moves row c < w).
-struct BatchPlan {
-    int blk[64];
-    int ext_row[64];
-    int ext_src[64];
-    int next;
-};
-
-// warp 0, once the pivot p of column c is known: compose c <-> p into the
-// plan (the rows >= w already displaced are searched by the whole warp)
-__device__ __forceinline__ void batch_plan_step(BatchPlan &s, int c, int p, int w, int lane)
-{
-    const int ne = s.next;
-    unsigned hit = 0;
-    for (int e0 = 0; e0 < ne; e0 += 32) {
-        const unsigned b = __ballot_sync(0xffffffffu, e0 + lane < ne && s.ext_row[e0 + lane] == p);
-        if (b && !hit) hit = (unsigned)(e0 + __ffs(b));  // index + 1
-    }
-    if (lane == 0) {
-        const int xc = s.blk[c];
-        if (p < w) {
-            s.blk[c] = s.blk[p];
-            s.blk[p] = xc;
-        } else if (p != c) {
-            int e = (int)hit - 1;
-            if (!hit) {
-                e = ne;
-                s.ext_row[e] = p;
-                s.ext_src[e] = p;
-                s.next = e + 1;
-            }
-            s.blk[c] = s.ext_src[e];
-            s.ext_src[e] = xc;
-        }
-    }
-    __syncwarp();
-}
-
 // blocked LU in global memory (L2-resident), panel of pw columns in shared memory
 __device__ void batch_solve_blocked(double *A, long ld, int n, int nrhs, int pw, double *P, double *U, int *piv,
                                     double *dinv, BatchPlan &plan, int *info)

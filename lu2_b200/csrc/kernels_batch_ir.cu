@@ -81,9 +81,15 @@ __device__ void ir_factor_smem(float *F, int n, int fs, int *piv, int *first_zer
 }
 
 // FP32 factorization of F (n x n, stride n) in global memory, panel of pw
-// columns staged in shared memory (P: rows x (pw+1), U: pw x 64)
+// columns staged in shared memory (P: rows x (pw+1), U: pw x 64).  The panel
+// is factored by the first NWP warps (up to 4), thread pt owning the panel
+// rows c + pt + k S (S = 32 NWP) for both the pivot search of column c and
+// the rank-1 step of column c - 1, with two named barriers of the S threads
+// per column; warp 0 composes the panel's row exchanges into one plan, which
+// the columns left of the panel (full-width exchanges) and the right part
+// then apply with independent loads instead of one dependent swap per pivot.
 __device__ void ir_factor_blocked(float *F, int n, int pw, float *P, float *U, int *piv, float *dinv,
-                                  int *first_zero, double *s_v, int *s_i)
+                                  int *first_zero, double *s_v, int *s_i, BatchPlan &plan)
 {
     const int T = blockDim.x, tid = threadIdx.x;
     const int ps = pw + 1;  // odd panel row stride: a column's rows fall in distinct banks
@@ -94,80 +100,104 @@ __device__ void ir_factor_blocked(float *F, int n, int pw, float *P, float *U, i
             P[r * ps + c] = F[(size_t)(k0 + r) * n + k0 + c];
         }
         __syncthreads();
-        for (int c = 0; c < w; c++) {
-            double v = -1.0;
-            int p = INT_MAX;
-            for (int r = c + tid; r < rows; r += T) {
-                const double a = fabsf(P[r * ps + c]);
-                if (a > v) {
-                    v = a;
-                    p = r;
-                }
+        const int nwp = min(4, T >> 5), S = 32 * nwp;
+        if (tid < S) {
+            const int lane = tid & 31, pw_ = tid >> 5;
+            if (tid < 32) {
+                for (int q = lane; q < w; q += 32) plan.blk[q] = q;
+                if (lane == 0) plan.next = 0;
+                __syncwarp();
             }
-            ir_block_argmax(v, p, s_v, s_i);
-            if (p == INT_MAX) p = c;
-            if (tid == 0) piv[k0 + c] = k0 + p;
-            if (p != c)
-                for (int j = tid; j < w; j += T) {
-                    const float t = P[c * ps + j];
-                    P[c * ps + j] = P[p * ps + j];
-                    P[p * ps + j] = t;
+            for (int c = 0; c < w; c++) {
+                double v = -1.0;
+                int p = INT_MAX;
+                for (int r = c + tid; r < rows; r += S) {
+                    const double a = fabsf(P[r * ps + c]);
+                    if (a > v) {
+                        v = a;
+                        p = r;
+                    }
                 }
-            __syncthreads();
-            const float d = P[c * ps + c];
-            const bool zero = (d == 0.f);
-            if (zero && !*first_zero && tid == 0) *first_zero = k0 + c + 1;
-            const float inv = zero ? 1.f : 1.f / d;
-            if (tid == 0) dinv[c] = inv;
-            if (!zero)
-                for (int j = c + 1 + tid; j < w; j += T) P[c * ps + j] *= inv;
-            __syncthreads();
-            if (!zero) {
-                const int wj = w - c - 1, hr = rows - c - 1;
-                for (int idx = tid; idx < hr * wj; idx += T) {
-                    const int r = c + 1 + idx / wj, j = c + 1 + idx % wj;
-                    P[r * ps + j] -= P[r * ps + c] * P[c * ps + j];
+                warp_argmax(v, p);
+                if (lane == 0) {
+                    s_v[pw_] = v;
+                    s_i[pw_] = p;
                 }
+                asm volatile("bar.sync 1, %0;" ::"r"(S) : "memory");
+                v = s_v[0];
+                p = s_i[0];
+                for (int q = 1; q < nwp; q++)
+                    if (argmax_better(s_v[q], s_i[q], v, p)) {
+                        v = s_v[q];
+                        p = s_i[q];
+                    }
+                if (p == INT_MAX) p = c;
+                if (tid < 32) {
+                    if (lane == 0) piv[k0 + c] = k0 + p;
+                    if (p != c)
+                        for (int j = lane; j < w; j += 32) {
+                            const float t = P[c * ps + j];
+                            P[c * ps + j] = P[p * ps + j];
+                            P[p * ps + j] = t;
+                        }
+                    __syncwarp();
+                    const float d = P[c * ps + c];
+                    const bool zero = (d == 0.f);
+                    const float inv = zero ? 1.f : 1.f / d;
+                    if (lane == 0) dinv[c] = inv;
+                    __syncwarp();  // every lane has read the pivot before the row is scaled
+                    if (!zero)
+                        for (int j = c + 1 + lane; j < w; j += 32) P[c * ps + j] *= inv;
+                    batch_plan_step(plan, c, p, w, lane);
+                }
+                asm volatile("bar.sync 1, %0;" ::"r"(S) : "memory");
+                const bool zero = (P[c * ps + c] == 0.f);
+                if (zero && tid == 0 && !*first_zero) *first_zero = k0 + c + 1;
+                if (!zero)
+                    for (int r = c + 1 + tid; r < rows; r += S) {
+                        const float l = P[r * ps + c];
+                        for (int j = c + 1; j < w; j++) P[r * ps + j] -= l * P[c * ps + j];
+                    }
             }
-            __syncthreads();
         }
+        __syncthreads();
         for (int idx = tid; idx < rows * w; idx += T) {
             const int r = idx / w, c = idx - r * w;
             F[(size_t)(k0 + r) * n + k0 + c] = P[r * ps + c];
         }
-        // exchanges of the earlier panels' columns (full-width rows), one thread per column
-        for (int j = tid; j < k0; j += T)
-            for (int c = 0; c < w; c++) {
-                const int p = piv[k0 + c];
-                if (p != k0 + c) {
-                    float *a = F + (size_t)(k0 + c) * n + j, *b = F + (size_t)p * n + j;
-                    const float t = *a;
-                    *a = *b;
-                    *b = t;
-                }
-            }
-        __syncthreads();
-        // right part: exchanges, then U' rows of the block (one thread per column)
-        const int cs = k0 + w;
-        for (int j = cs + tid; j < n; j += T) {
+        // the composed exchanges on the columns left of the panel (full-width
+        // rows) and, with the unit-lower solve and the 1/pivot scaling, on the
+        // right part, one thread per column: every gather first (16 loads in
+        // flight), then the displaced rows (read before the rows they come
+        // from are rewritten, written after every gather, since a gathered row
+        // may be one of them), then the panel's rows
+        const int cs = k0 + w, ne = plan.next, nleft = k0, ncols = k0 + (n - cs);
+        for (int jj = tid; jj < ncols; jj += T) {
+            const int j = jj < nleft ? jj : cs + (jj - nleft);
             float x[64];
-            for (int c = 0; c < w; c++) {
-                const int p = piv[k0 + c];
-                float *rc = F + (size_t)(k0 + c) * n + j;
-                float vc = *rc;
-                if (p != k0 + c) {
-                    float *rp = F + (size_t)p * n + j;
-                    const float vp = *rp;
-                    *rp = vc;
-                    vc = vp;
+            for (int q0 = 0; q0 < w; q0 += 16) {
+                float v[16];
+#pragma unroll
+                for (int u = 0; u < 16; u++) v[u] = q0 + u < w ? F[(size_t)(k0 + plan.blk[q0 + u]) * n + j] : 0.f;
+#pragma unroll
+                for (int u = 0; u < 16; u++)
+                    if (q0 + u < w) x[q0 + u] = v[u];
+            }
+            for (int e0 = 0; e0 < ne; e0 += 16) {
+                float v[16];
+#pragma unroll
+                for (int u = 0; u < 16; u++)
+                    v[u] = e0 + u < ne ? F[(size_t)(k0 + plan.ext_src[e0 + u]) * n + j] : 0.f;
+#pragma unroll
+                for (int u = 0; u < 16; u++)
+                    if (e0 + u < ne) F[(size_t)(k0 + plan.ext_row[e0 + u]) * n + j] = v[u];
+            }
+            if (jj >= nleft)
+                for (int r = 0; r < w; r++) {
+                    float s = x[r];
+                    for (int l = 0; l < r; l++) s -= P[r * ps + l] * x[l];
+                    x[r] = s * dinv[r];
                 }
-                x[c] = vc;
-            }
-            for (int r = 0; r < w; r++) {
-                float s = x[r];
-                for (int l = 0; l < r; l++) s -= P[r * ps + l] * x[l];
-                x[r] = s * dinv[r];
-            }
             for (int c = 0; c < w; c++) F[(size_t)(k0 + c) * n + j] = x[c];
         }
         __syncthreads();
@@ -343,6 +373,7 @@ __global__ void batch_ir_kernel(double *data, const BatchSys *sys, const long lo
     __shared__ int s_i[32];
     __shared__ int s_next, s_zero, s_done;
     __shared__ float s_dinv[64];
+    __shared__ BatchPlan s_plan;
     __shared__ double s_red[32 * (2 * IR_MAX_RHS + 1)];
     __shared__ double s_rmax[IR_MAX_RHS], s_xmax[IR_MAX_RHS], s_bmax[IR_MAX_RHS], s_anorm;
     const int T = blockDim.x, tid = threadIdx.x;
@@ -376,7 +407,7 @@ __global__ void batch_ir_kernel(double *data, const BatchSys *sys, const long lo
         if (in_smem)
             ir_factor_smem(F, n, fs, piv, &s_zero, s_v, s_i);
         else
-            ir_factor_blocked(F, n, pw, ism, ism + (size_t)n * (pw + 1), piv, s_dinv, &s_zero, s_v, s_i);
+            ir_factor_blocked(F, n, pw, ism, ism + (size_t)n * (pw + 1), piv, s_dinv, &s_zero, s_v, s_i, s_plan);
         __syncthreads();
         int it = 0;
         if (s_zero == 0) {

@@ -228,6 +228,47 @@ struct BatchSys {
     long long off;
     int n, nrhs, ld, pw;
 };
+// The row exchanges of one panel composed into a plan: U row q takes the
+// content of panel row blk[q], and the rows ext_row[e] >= w take the old
+// content of U row ext_src[e] (every displaced row receives a U row, since
+// each exchange moves row c < w).
+struct BatchPlan {
+    int blk[64];
+    int ext_row[64];
+    int ext_src[64];
+    int next;
+};
+
+// warp 0, once the pivot p of column c is known: compose c <-> p into the
+// plan (the rows >= w already displaced are searched by the whole warp)
+__device__ __forceinline__ void batch_plan_step(BatchPlan &s, int c, int p, int w, int lane)
+{
+    const int ne = s.next;
+    unsigned hit = 0;
+    for (int e0 = 0; e0 < ne; e0 += 32) {
+        const unsigned b = __ballot_sync(0xffffffffu, e0 + lane < ne && s.ext_row[e0 + lane] == p);
+        if (b && !hit) hit = (unsigned)(e0 + __ffs(b));  // index + 1
+    }
+    if (lane == 0) {
+        const int xc = s.blk[c];
+        if (p < w) {
+            s.blk[c] = s.blk[p];
+            s.blk[p] = xc;
+        } else if (p != c) {
+            int e = (int)hit - 1;
+            if (!hit) {
+                e = ne;
+                s.ext_row[e] = p;
+                s.ext_src[e] = p;
+                s.next = e + 1;
+            }
+            s.blk[c] = s.ext_src[e];
+            s.ext_src[e] = xc;
+        }
+    }
+    __syncwarp();
+}
+
 // dynamic shared memory a CTA of the batched launch may use
 constexpr size_t BATCH_SMEM_MAX = 220 * 1024;
 // blocked path: panel row stride pw + BATCH_PANEL_PAD (odd, so that lanes on
