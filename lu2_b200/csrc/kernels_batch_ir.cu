@@ -23,54 +23,46 @@
 
 namespace lu2gpu {
 
-__device__ __forceinline__ void ir_block_argmax(double &v, int &i, double *s_v, int *s_i)
-{
-    warp_argmax(v, i);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    if (lane == 0) {
-        s_v[warp] = v;
-        s_i[warp] = i;
-    }
-    __syncthreads();
-    v = lane < nw ? s_v[lane] : -1.0;
-    i = lane < nw ? s_i[lane] : INT_MAX;
-    warp_argmax(v, i);
-    __syncthreads();
-}
-
-// FP32 factorization of F (n x n, stride n) held in shared memory
-__device__ void ir_factor_smem(float *F, int n, int fs, int *piv, int *first_zero, double *s_v, int *s_i)
+// FP32 factorization of F (n x n, stride fs) held in shared memory: per
+// column warp 0 alone (warp-synchronously) searches the pivot, exchanges the
+// full rows and scales the pivot row, then after one barrier every thread
+// takes part in the rank-1 update -- two barriers per column
+__device__ void ir_factor_smem(float *F, int n, int fs, int *piv, int *first_zero)
 {
     const int T = blockDim.x, tid = threadIdx.x;
     for (int k = 0; k < n; k++) {
-        double v = -1.0;
-        int p = INT_MAX;
-        for (int r = k + tid; r < n; r += T) {
-            const double a = fabsf(F[r * fs + k]);
-            if (a > v) {
-                v = a;
-                p = r;
+        if (tid < 32) {
+            const int lane = tid;
+            double v = -1.0;
+            int p = INT_MAX;
+            for (int r = k + lane; r < n; r += 32) {
+                const double a = fabsf(F[r * fs + k]);
+                if (a > v) {
+                    v = a;
+                    p = r;
+                }
+            }
+            warp_argmax(v, p);
+            if (p == INT_MAX) p = k;
+            if (lane == 0) piv[k] = p;
+            if (p != k)
+                for (int c = lane; c < n; c += 32) {
+                    const float t = F[k * fs + c];
+                    F[k * fs + c] = F[p * fs + c];
+                    F[p * fs + c] = t;
+                }
+            __syncwarp();
+            const float d = F[k * fs + k];
+            __syncwarp();  // every lane has read the pivot before the row is scaled
+            if (d != 0.f) {
+                const float inv = 1.f / d;
+                for (int c = k + 1 + lane; c < n; c += 32) F[k * fs + c] *= inv;
+            } else if (lane == 0 && !*first_zero) {
+                *first_zero = k + 1;
             }
         }
-        ir_block_argmax(v, p, s_v, s_i);
-        if (p == INT_MAX) p = k;
-        if (tid == 0) piv[k] = p;
-        if (p != k)
-            for (int c = tid; c < n; c += T) {
-                const float t = F[k * fs + c];
-                F[k * fs + c] = F[p * fs + c];
-                F[p * fs + c] = t;
-            }
         __syncthreads();
-        const float d = F[k * fs + k];
-        if (d == 0.f) {
-            if (!*first_zero && tid == 0) *first_zero = k + 1;
-            __syncthreads();
-            continue;
-        }
-        const float inv = 1.f / d;
-        for (int c = k + 1 + tid; c < n; c += T) F[k * fs + c] *= inv;
-        __syncthreads();
+        if (F[k * fs + k] == 0.f) continue;  // (uniform: every thread reads the same pivot)
         const int w = n - k - 1;
         for (int idx = tid; idx < w * w; idx += T) {
             const int r = k + 1 + idx / w, c = k + 1 + idx % w;
@@ -405,7 +397,7 @@ __global__ void batch_ir_kernel(double *data, const BatchSys *sys, const long lo
         }
         __syncthreads();
         if (in_smem)
-            ir_factor_smem(F, n, fs, piv, &s_zero, s_v, s_i);
+            ir_factor_smem(F, n, fs, piv, &s_zero);
         else
             ir_factor_blocked(F, n, pw, ism, ism + (size_t)n * (pw + 1), piv, s_dinv, &s_zero, s_v, s_i, s_plan);
         __syncthreads();
