@@ -51,3 +51,29 @@ def test_header_status_codes_match_binding():
     for name, val in [("LU2GPU_ERR_ARG", "(-1)"), ("LU2GPU_ERR_NODEV", "(-5)"), ("LU2GPU_PIVOT_REF", "0"),
                       ("LU2GPU_PIVOT_PARTIAL", "1")]:
         assert "#define %s %s" % (name, val) in text
+
+
+def test_exit_hook_closes_batches_before_contexts():
+    """The binding's exit hook closes every batch still open before any
+    context (a batch's memory and streams belong to its context), and
+    finalizers run during interpreter shutdown do nothing."""
+    from lu2_b200 import lu2
+
+    order = []
+
+    class Fake:
+        def __init__(self, name):
+            self.name = name
+
+        def close(self):
+            order.append(self.name)
+
+    ctx, batch = Fake("context"), Fake("batch")
+    lu2._LIVE_CONTEXTS.add(ctx)
+    lu2._LIVE_BATCHES.add(batch)
+    try:
+        lu2._close_live()
+    finally:
+        lu2._LIVE_CONTEXTS.discard(ctx)
+        lu2._LIVE_BATCHES.discard(batch)
+    assert order == ["batch", "context"]
