@@ -258,14 +258,15 @@ __device__ void batch_solve_blocked(double *A, long ld, int n, int nrhs, int pw,
                 U[l * BATCH_U_STRIDE + c] = (l < w && c < cw) ? A[(size_t)(k0 + l) * ld + c0 + c] : 0.0;
             }
             __syncthreads();
-            constexpr int HALVES = BATCH_U_CHUNK / 32;  // 32-column halves of a warp's 16-row strip
-            const int units = ((h + 15) >> 4) * HALVES;
+            constexpr int UNB = BATCH_UNIT_COLS / 8;           // 8-column MMA blocks of a unit
+            constexpr int PARTS = BATCH_U_CHUNK / BATCH_UNIT_COLS;  // units across a chunk's 16-row strip
+            const int units = ((h + 15) >> 4) * PARTS;
             for (int u = warp; u < units; u += nwarps) {
-                const int r0 = (u / HALVES) << 4, cb = (u % HALVES) << 5;  // strip rows r0.., chunk columns cb..cb+31
+                const int r0 = (u / PARTS) << 4, cb = (u % PARTS) * BATCH_UNIT_COLS;  // strip rows r0.., chunk columns cb..
                 const int rl = r0 + g, rh = rl + 8;                // rows (of the trailing block) of c0,c1 / c2,c3
-                double acc[4][4];
+                double acc[UNB][4];
 #pragma unroll
-                for (int j = 0; j < 4; j++) {
+                for (int j = 0; j < UNB; j++) {
                     const int col = cb + 8 * j + 2 * t;  // chunk column of c0 / c2
 #pragma unroll
                     for (int hh = 0; hh < 2; hh++) {
@@ -294,14 +295,14 @@ __device__ void batch_solve_blocked(double *A, long ld, int n, int nrhs, int pw,
                     const double a2 = (rl < h && kb < w) ? -pl[kb] : 0.0;
                     const double a3 = (rh < h && kb < w) ? -ph[kb] : 0.0;
 #pragma unroll
-                    for (int j = 0; j < 4; j++) {
+                    for (int j = 0; j < UNB; j++) {
                         const double b0 = U[ka * BATCH_U_STRIDE + cb + 8 * j + g];
                         const double b1 = U[kb * BATCH_U_STRIDE + cb + 8 * j + g];
                         batch_dmma(acc[j], a0, a1, a2, a3, b0, b1);
                     }
                 }
 #pragma unroll
-                for (int j = 0; j < 4; j++) {
+                for (int j = 0; j < UNB; j++) {
                     const int col = cb + 8 * j + 2 * t;
 #pragma unroll
                     for (int hh = 0; hh < 2; hh++) {

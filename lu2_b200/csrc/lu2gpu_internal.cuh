@@ -274,6 +274,7 @@ constexpr size_t BATCH_SMEM_MAX = 220 * 1024;
 // blocked path: panel row stride pw + BATCH_PANEL_PAD (odd, so that lanes on
 // consecutive rows hit different banks); the U chunk of the update
 constexpr int BATCH_PANEL_PAD = 1;
+constexpr int BATCH_UNIT_COLS = 32;  // columns of a warp's update tile, 16 rows x this (16 measured slower: 41.3 vs 40.9 ms)
 constexpr int BATCH_U_CHUNK = 64;  // columns of U12 staged per update step (128 measured slower: 42.3 vs 40.9 ms)
 constexpr int BATCH_U_STRIDE = BATCH_U_CHUNK + 4;  // B-fragment reads of a half-warp on distinct banks
 // shared-memory doubles a CTA needs for the systems sys[0..count) with panel width pw
