@@ -2652,7 +2652,7 @@ static int factor32_serial(lu2gpu_ctx *c, const View32 &v, int n, int nb, int mo
 // next panel is factored on a second stream while the rest of the update runs.
 // The persistent update kernel is held to sms - R CTAs (one per SM, by its
 // shared memory), which leaves R SMs for the panel's leaf CTAs (R = the
-// fewest CTAs whose FP32 slab fits, at least 24).  Step k+1's right part waits
+// fewest CTAs whose FP32 slab fits, at least 32).  Step k+1's right part waits
 // for that panel: its row exchanges cross the columns the update wrote.
 // Serial when phase timing is on (so the phase split stays meaningful), for
 // small n, or with LU2GPU_LOOKAHEAD=0.
@@ -2661,7 +2661,10 @@ static int factor32_or_fail(lu2gpu_ctx *c, int n, float *a, long ld, int nb, int
     View32 v{a, ld, n, n, 0};
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-    const int R = std::max(24, leaf_min_ctas(n, sizeof(float)));
+    // SMs held for the panel beside the update (LU2GPU_PANEL_SMS, read per
+    // call; N=65536 BF16 factor: 24 SMs 1.002 s, 32 0.996 s, 48 1.018 s)
+    const char *ps = getenv("LU2GPU_PANEL_SMS");
+    const int R = std::max(ps ? atoi(ps) : 32, leaf_min_ctas(n, sizeof(float)));
     const char *env = getenv("LU2GPU_LOOKAHEAD");
     const bool lookahead = !c->timing && n >= 4 * nb && 2 * R < sms && !(env && env[0] == '0');
     if (!lookahead) return factor32_serial(c, v, n, nb, mode);
